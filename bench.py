@@ -1,0 +1,309 @@
+#!/usr/bin/env python
+"""Benchmark of the DG-BGK pseudo-time sweep on B200.
+
+One "step" is one pseudo-time step of the reference time loop (ADVNCE,
+src/advnce.f90:220-449) over the whole case.  The default workload is the
+supersonic channel: [-5,15]x[-5,5] as 200x100 quads (39 800 P1 triangles)
+minus a unit-square obstacle, 24 x 48 velocities (1.3755e8 DOFs), Mach 2,
+Kn 0.05, f stored in FP32 with FP64 moments and residual norms.  The metric
+is DOF-updates/s = 3*NELEM*VNPNT*steps / device time of the time loop.
+
+Arms:
+  --impl ours       : the sm_100a library through its C ABI.
+  --impl reference  : the reference algorithm on the host cores (the oracle,
+                      a C++ restatement of the Fortran: it cannot be compiled
+                      here), FP32 like the shipped build, all host threads.
+
+Multi-GPU (torchrun): the step does not shard in this build (velocity-space
+sharding is future work), so N ranks run N independent replicas; value is
+the aggregate DOF-updates/s over all ranks with the time taken as the max
+over ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "dg-bgk_b200"))
+
+METRIC = "time-to-steady-state (res 1e-8) and DOF-updates/s: plain FP64 vs FP32+warm-start, 1 B200"
+UNIT = "DOF-updates/s"
+
+
+def args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="channel", choices=["channel", "cavity", "large"])
+    ap.add_argument("--precision", type=int, default=32, choices=[32, 64])
+    ap.add_argument("--no-fp64", action="store_true", help="skip the plain-FP64 comparison leg")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def make_case(name):
+    import dgbgk
+    return {"channel": dgbgk.config2, "cavity": dgbgk.config1, "large": dgbgk.config5}[name]()
+
+
+def workload(case, prec):
+    m = case.mesh
+    return (f"{case.name}: {m.nelem} P1 elements x {case.rorder}x{case.torder} velocities = {case.dofs} DOFs, "
+            f"Mach {case.info.get('mach')}, Kn {case.info.get('kn')}, f in FP{prec}")
+
+
+# ------------------------------------------------------------------ dist ----
+class Dist:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+            import torch
+            import torch.distributed as dist
+            backend = "nccl" if torch.cuda.is_available() else "gloo"
+            if backend == "nccl":
+                torch.cuda.set_device(self.local)
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+            self.pg = dist
+            self.backend = backend
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, x):
+        if not self.pg:
+            return x
+        import torch
+        dev = f"cuda:{self.local}" if self.backend == "nccl" else "cpu"
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ---------------------------------------------------------------- clocks ----
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = str(gpu_index)
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-i", self.idx, "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        rows = [r for r in self.rows if len(r) >= 9]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs (of measured)"
+    return 6650.0, "profiling-recipe fallback 6.65 TB/s (of fallback)"
+
+
+def ncu_traffic(case_name, prec):
+    """dram bytes per sweep launch from the committed ncu summary, if it
+    covers this workload."""
+    p = os.path.join(ROOT, "profiles", "sweep_traffic.json")
+    if not os.path.exists(p):
+        return None
+    d = json.load(open(p))
+    e = d.get(f"{case_name}/fp{prec}")
+    return None if e is None else e.get("dram_bytes_per_launch")
+
+
+def cpu_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def oracle_step_rate(case, nsteps, threads, warmup=0):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from pyoracle import Oracle
+    o = Oracle.from_case(case, prec=32, threads=threads)
+    i = case.init
+    o.inicon2(i["T1"], i["P1"], i["U0"], i["V0"])
+    if warmup:
+        o.advance(warmup)
+    t = time.perf_counter()
+    o.advance(nsteps)
+    dt = time.perf_counter() - t
+    o.close()
+    return case.dofs * nsteps / dt, dt
+
+
+# ------------------------------------------------------------- our arm ----
+def run_ours(a, d):
+    import numpy as np
+    import torch
+    from dgbgk import Solver
+
+    torch.cuda.set_device(d.local)
+    case = make_case(a.config)
+    s = Solver.from_case(case, precision=a.precision, device=d.local)
+    s.init_case()
+    s.advance(max(a.warmup, 3))
+    info = s.info()
+    clocks = Clocks(d.local)
+    d.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    r = s.advance(a.steps)
+    torch.cuda.synchronize()
+    ck = clocks.stop()
+    d.barrier()
+    t_ms = d.max(s.last_ms())
+    assert r["steps"] == a.steps
+    dof_rate = d.world * case.dofs * a.steps / (t_ms * 1e-3)
+
+    # dominant kernel, timed live with CUDA events on the library's stream
+    kms = s.profile(5)
+    names = ["k_moments", "k_wall", "k_sweep", "k_resid"]
+    sf = 4 if a.precision == 32 else 8
+    alg_bytes = 2 * sf * case.dofs  # one read + one write of f per DOF-update
+    peak, peak_src = peaks()
+    achieved = alg_bytes / (kms[2] * 1e-3) / 1e9
+    traffic = ncu_traffic(case.name, a.precision)
+    step_gbs = dof_rate / d.world * 2 * sf / 1e9
+
+    out = {"metric": METRIC, "value": dof_rate, "unit": UNIT, "n_gpus": d.world, "steps": a.steps,
+           "warmup": a.warmup, "ms_per_step": t_ms / a.steps, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32" if a.precision == 32 else "f64",
+           "data": "synthetic (generated mesh and velocity grid; free-stream initial state)",
+           "config": {"workload": workload(case, a.precision), "nelem": case.mesh.nelem,
+                      "vnpnt": case.rorder * case.torder, "dofs": case.dofs,
+                      "tile_elems": info["tile_elems"], "max_halo": info["max_halo"],
+                      "l2": f"inputs larger than L2: each f buffer is {case.dofs * sf / 1e6:.0f} MB",
+                      "parallelism": f"replicas x{d.world}" if d.world > 1 else "single GPU"},
+           "roofline": {"bound": "hbm", "kernel": "k_sweep", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                        "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
+                        "alg_bytes_per_launch": alg_bytes,
+                        "kernel_ms": dict(zip(names, [float(x) for x in kms])),
+                        "step_frac": step_gbs / peak},
+           "clocks": ck,
+           "gpu_launches": a.steps * (4 if (case.mesh.bsido[:, 3] == 4).any() else 3)}
+    del s
+    # plain FP64 path on the same workload
+    if not a.no_fp64 and a.precision == 32:
+        s64 = Solver.from_case(case, precision=64, device=d.local)
+        s64.init_case()
+        s64.advance(max(a.warmup, 3))
+        d.barrier()
+        r64 = s64.advance(a.steps)
+        t64 = d.max(s64.last_ms())
+        k64 = s64.profile(3)
+        out["fp64"] = {"value": d.world * case.dofs * a.steps / (t64 * 1e-3), "ms_per_step": t64 / a.steps,
+                       "sweep_gbs": 16 * case.dofs / (k64[2] * 1e-3) / 1e9,
+                       "kernel_ms": dict(zip(names, [float(x) for x in k64]))}
+        out["fp32_over_fp64_per_step"] = out["value"] / out["fp64"]["value"]
+        del s64
+    # end to end through the C ABI with host buffers
+    if not a.no_e2e:
+        s = Solver.from_case(case, precision=a.precision, device=d.local)
+        s.init_case()
+        host = torch.empty((case.mesh.nelem, case.rorder * case.torder, 3),
+                           dtype=torch.float32 if a.precision == 32 else torch.float64).pin_memory()
+        hv = host.numpy()
+        hv[...] = s.get_state(hv.dtype.type)
+        s.advance(2)
+        d.barrier()
+        t0 = time.perf_counter()
+        s.set_state(hv)                  # H2D of DISNF(3,V,E) + layout change
+        s.advance(a.steps)
+        hv[...] = s.get_state(hv.dtype.type)  # D2H of the advanced DISNF
+        t1 = time.perf_counter()
+        te = d.max(t1 - t0)
+        nb = host.numel() * host.element_size()
+        out["e2e"] = {"value": d.world * case.dofs * a.steps / te, "unit": UNIT,
+                      "h2d_bytes_per_step": nb / a.steps, "d2h_bytes_per_step": nb / a.steps,
+                      "note": f"set_state + advance({a.steps}) + get_state per call, pinned host DISNF"}
+        del s
+    if d.rank == 0 and d.world == 1 and not a.no_cpu:
+        thr = cpu_threads()
+        rate, secs = oracle_step_rate(case, 1, thr)
+        out["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": thr, "kind": "port",
+                               "sample": f"1 full pseudo-time step of {case.name} (FP32, {secs:.1f} s, "
+                                         f"{thr} OpenMP threads)"}
+    return out
+
+
+def run_reference(a, d):
+    if d.rank != 0:
+        return None
+    case = make_case(a.config)
+    thr = cpu_threads()
+    rate, secs = oracle_step_rate(case, a.steps, thr, warmup=a.warmup)
+    return {"impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": d.world,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": secs * 1e3 / a.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (generated mesh and velocity grid; free-stream initial state)",
+            "config": {"workload": workload(case, 32), "dofs": case.dofs},
+            "cpu_baseline": {"value": rate, "unit": UNIT, "cores": thr, "kind": "port",
+                             "sample": f"{a.steps} full pseudo-time steps of {case.name} after {a.warmup} warm-up "
+                                       f"steps (FP32, {thr} OpenMP threads)"},
+            "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    a = args()
+    d = Dist()
+    try:
+        out = run_reference(a, d) if a.impl == "reference" else run_ours(a, d)
+        if d.rank == 0 and out is not None:
+            print(json.dumps(out), flush=True)
+    finally:
+        d.close()
+
+
+if __name__ == "__main__":
+    main()

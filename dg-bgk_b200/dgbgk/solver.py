@@ -1,0 +1,233 @@
+"""Python host side of the drop-in: the same steps DG_LIN_CONVEC takes around
+ADVNCE (src/dg_lin_convec.f90:96-206) -- setup arrays, initial condition,
+time loop, nodal output -- with every compute call going through the C ABI
+of lib/libdgbgk.so.
+"""
+import ctypes
+from ctypes import POINTER, c_double, c_float, c_int, c_void_p
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, lib, ptr
+
+
+@dataclass
+class Setup:
+    """The reference's setup arrays (src/dg_lin_convec.f90:96-125)."""
+    nside: int
+    iside: np.ndarray  # (S,8) int32
+    nx: np.ndarray
+    ny: np.ndarray
+    el: np.ndarray
+    geome: np.ndarray  # (E,7)
+    relen: np.ndarray
+    mmat: np.ndarray   # (E,3)
+    cmmat: np.ndarray  # (E,3,3) as CMMAT(3,3,E): [e, j, i]
+    rsido: np.ndarray  # (B,3)
+
+
+def setup_mesh(intma, coord, bsido):
+    """GETSID, NORMAL, GETGEO, GETLEN, GETMAT/CONMAT, GETNOR on the host."""
+    intma = np.ascontiguousarray(intma, dtype=np.int32)
+    coord = np.ascontiguousarray(coord, dtype=np.float64)
+    bsido = np.ascontiguousarray(bsido, dtype=np.int32)
+    E, NP, B = intma.shape[0], coord.shape[0], bsido.shape[0]
+    mx = 2 * (E + B)
+    iside = np.zeros((mx, 8), dtype=np.int32)
+    nx = np.zeros(mx)
+    ny = np.zeros(mx)
+    el = np.zeros(mx)
+    geome = np.zeros((E, 7))
+    relen = np.zeros(E)
+    mmat = np.zeros((E, 3))
+    cmmat = np.zeros((E, 3, 3))
+    rsido = np.zeros((max(B, 1), 3))
+    ns = c_int(0)
+    check(lib().dgbgk_setup_mesh(E, NP, B, ptr(intma, c_int), ptr(coord), ptr(bsido, c_int), ctypes.byref(ns),
+                                 ptr(iside, c_int), ptr(nx), ptr(ny), ptr(el), ptr(geome), ptr(relen), ptr(mmat),
+                                 ptr(cmmat), ptr(rsido)))
+    S = ns.value
+    return Setup(S, iside[:S].copy(), nx[:S].copy(), ny[:S].copy(), el[:S].copy(), geome, relen, mmat, cmmat,
+                 rsido[:B].copy())
+
+
+def vspace(rorder, torder, eta, w):
+    """VSPACE: VCORD(3,V) and SUMWEIGHT."""
+    eta = np.ascontiguousarray(eta, dtype=np.float64)
+    w = np.ascontiguousarray(w, dtype=np.float64)
+    vc = np.zeros((rorder * torder, 3))
+    sw = c_double(0)
+    check(lib().dgbgk_vspace_build(rorder, torder, ptr(eta), ptr(w), ptr(vc), ctypes.byref(sw)))
+    return vc, sw.value
+
+
+class Solver:
+    """One case on one GPU.  Arrays use the reference layouts: DISNF is
+    (NELEM, VNPNT, 3) C-order == DISNF(3,VNPNT,NELEM) column-major."""
+
+    def __init__(self, intma, coord, bsido, setup, vcord, sumweight, rorder, torder, rv, *, immat=1, csafm=0.5,
+                 alpha=1.0, rgas=1.0, molar_mass=6.022e26, diameter=1.0, cinf=(0, 0, 0, 0), precision=64,
+                 wall_velocity=None, tile_elems=0, device=0):
+        L = lib()
+        self._keep = []
+
+        def keep(a, dt=np.float64):
+            a = np.ascontiguousarray(a, dtype=dt)
+            self._keep.append(a)
+            return a
+
+        intma = keep(intma, np.int32)
+        coord = keep(coord)
+        bsido = keep(bsido, np.int32)
+        self.E, self.NP, self.B = intma.shape[0], coord.shape[0], bsido.shape[0]
+        self.V = rorder * torder
+        m = _lib.Mesh()
+        m.nelem, m.npoin, m.nboun, m.nside = self.E, self.NP, self.B, setup.nside
+        m.intma = ptr(intma, c_int)
+        m.coord = ptr(coord)
+        m.bsido = ptr(bsido, c_int) if self.B else None
+        m.iside = ptr(keep(setup.iside, np.int32), c_int)
+        m.nx = ptr(keep(setup.nx))
+        m.ny = ptr(keep(setup.ny))
+        m.el = ptr(keep(setup.el))
+        m.geome = ptr(keep(setup.geome))
+        m.relen = ptr(keep(setup.relen))
+        m.mmat = ptr(keep(setup.mmat))
+        m.cmmat = ptr(keep(setup.cmmat))
+        m.rsido = ptr(keep(setup.rsido)) if self.B else None
+        vs = _lib.VSpace()
+        vs.rorder, vs.torder = rorder, torder
+        vs.vcord = ptr(keep(vcord))
+        vs.sumweight = sumweight
+        vs.rv = rv
+        p = _lib.Params()
+        L.dgbgk_default_params(ctypes.byref(p))
+        p.immat, p.csafm, p.alpha, p.rgas = immat, csafm, alpha, rgas
+        p.molar_mass, p.diameter = molar_mass, diameter
+        for i in range(4):
+            p.cinf[i] = cinf[i]
+        p.precision = precision
+        p.wall_velocity = ptr(keep(wall_velocity)) if wall_velocity is not None else None
+        p.tile_elems = tile_elems
+        p.device = device
+        h = c_void_p()
+        check(L.dgbgk_create(ctypes.byref(m), ctypes.byref(vs), ctypes.byref(p), ctypes.byref(h)))
+        self.h = h
+        self.precision = precision
+
+    @classmethod
+    def from_case(cls, case, precision=64, tile_elems=0, device=0):
+        from .cases import gll
+        m = case.mesh
+        st = setup_mesh(m.intma, m.coord, m.bsido)
+        eta, w = gll(case.rorder)
+        vc, sw = vspace(case.rorder, case.torder, eta, w)
+        s = cls(m.intma, m.coord, m.bsido, st, vc, sw, case.rorder, case.torder, case.rv, immat=case.immat,
+                csafm=case.csafm, alpha=case.alpha, rgas=case.rgas, molar_mass=case.molar_mass,
+                diameter=case.diameter, cinf=case.cinf, precision=precision, wall_velocity=m.wall_velocity,
+                tile_elems=tile_elems, device=device)
+        s.case = case
+        s.setup = st
+        s.vcord = vc
+        s.sumweight = sw
+        return s
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().dgbgk_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- state --------------------------------------------------------
+    def set_state(self, disnf):
+        if disnf.dtype == np.float32:
+            a = np.ascontiguousarray(disnf)
+            assert a.size == 3 * self.E * self.V
+            check(lib().dgbgk_set_state_f32(self.h, ptr(a, c_float)))
+        else:
+            a = np.ascontiguousarray(disnf, dtype=np.float64)
+            assert a.size == 3 * self.E * self.V
+            check(lib().dgbgk_set_state(self.h, ptr(a)))
+
+    def get_state(self, dtype=np.float64):
+        out = np.empty((self.E, self.V, 3), dtype=dtype)
+        if dtype == np.float32:
+            check(lib().dgbgk_get_state_f32(self.h, ptr(out, c_float)))
+        else:
+            check(lib().dgbgk_get_state(self.h, ptr(out)))
+        return out
+
+    def inicon2(self, T1, P1, U0, V0, node_scale=None):
+        sc = None if node_scale is None else np.ascontiguousarray(node_scale, dtype=np.float64)
+        check(lib().dgbgk_init_uniform(self.h, T1, P1, U0, V0, ptr(sc)))
+
+    def init_case(self):
+        from .cases import node_scale
+        c = self.case
+        i = c.init
+        self.inicon2(i["T1"], i["P1"], i["U0"], i["V0"], node_scale(c))
+
+    def init_maxwellian(self, n, u, v, t):
+        a = [np.ascontiguousarray(x, dtype=np.float64).reshape(-1) for x in (n, u, v, t)]
+        check(lib().dgbgk_init_maxwellian(self.h, *(ptr(x) for x in a)))
+
+    # -- time loop ----------------------------------------------------
+    def advance(self, nsteps, tol=0.0):
+        linf = np.zeros(max(nsteps, 1))
+        l2 = np.zeros(max(nsteps, 1))
+        dte = np.zeros(max(nsteps, 1))
+        done = c_int(0)
+        rc = lib().dgbgk_advance(self.h, nsteps, tol, ctypes.byref(done), ptr(linf), ptr(l2), ptr(dte))
+        n = done.value
+        res = {"steps": n, "res_linf": linf[:n], "res_l2": l2[:n], "dte": dte[:n]}
+        check(rc)
+        return res
+
+    def last_ms(self):
+        t = c_double(0)
+        check(lib().dgbgk_last_timing(self.h, ctypes.byref(t)))
+        return t.value
+
+    def profile(self, nsteps):
+        """Mean device ms per step of [moments, wall, sweep, residual]."""
+        ms = np.zeros(4)
+        check(lib().dgbgk_profile_steps(self.h, nsteps, ptr(ms)))
+        return ms
+
+    def set_residual_reference(self, r):
+        check(lib().dgbgk_set_residual_reference(self.h, r))
+
+    def residual_reference(self):
+        r = c_double(0)
+        check(lib().dgbgk_get_residual_reference(self.h, ctypes.byref(r)))
+        return r.value
+
+    # -- observables ----------------------------------------------------
+    def macros(self):
+        out = {k: np.zeros(self.NP) for k in ("nd", "rho", "u", "v", "ps", "temp")}
+        check(lib().dgbgk_get_macros(self.h, *(ptr(out[k]) for k in ("nd", "rho", "u", "v", "ps", "temp"))))
+        return out
+
+    def node_fields(self):
+        out = {k: np.zeros((self.E, 3)) for k in ("disnd", "disux", "disuy", "disps", "mu")}
+        check(lib().dgbgk_get_node_fields(self.h, *(ptr(out[k]) for k in ("disnd", "disux", "disuy", "disps", "mu"))))
+        return out
+
+    def wall_eta(self):
+        out = np.zeros(max(self.B, 1))
+        check(lib().dgbgk_get_wall_eta(self.h, ptr(out)))
+        return out[:self.B]
+
+    def info(self):
+        o = np.zeros(10, dtype=np.int32)
+        check(lib().dgbgk_info(self.h, ptr(o, c_int)))
+        keys = ["nelem", "npoin", "nboun", "nside", "vnpnt", "precision", "tile_elems", "tile_vels", "n_blocks",
+                "max_halo"]
+        return dict(zip(keys, (int(x) for x in o)))

@@ -1,0 +1,182 @@
+/*
+ * dgbgk.h -- C ABI of the B200 (sm_100a) implementation of the DG-BGK
+ * transport-plus-collision pseudo-time sweep.
+ *
+ * The library replaces the reference time step ADVNCE (src/advnce.f90:3-25,
+ * called once from src/dg_lin_convec.f90:185-206) and the output gather
+ * GETMAC (src/getmac.f90:3-127).  A host written in any language binds these
+ * entry points; the Fortran ISO_C_BINDING binding that DG_LIN_CONVEC would
+ * use is given in INTEGRATION.md.
+ *
+ * Conventions
+ *  - Every array argument is caller-owned host memory and is copied in or
+ *    out; the library owns all device memory.  No torch or CUDA types appear
+ *    in the signatures.
+ *  - Mesh arrays keep the reference's Fortran layout: column-major with the
+ *    reference's leading dimensions, 1-based node/element indices
+ *    (INTMA(3,NELEM), BSIDO(6,NBOUN), ISIDE(8,NSIDE) ...).  Reals are double.
+ *  - The distribution function keeps the reference layout
+ *    DISNF(3, VNPNT, NELEM), column-major (src/dg_lin_convec.f90:93).
+ *  - Status: 0 = success; a negative DGBGK_E* code otherwise, with a message
+ *    from dgbgk_last_error().  The library never calls exit().
+ *  - One host thread per handle; distinct handles may be used from distinct
+ *    threads.
+ */
+#ifndef DGBGK_H
+#define DGBGK_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DGBGK_OK 0
+#define DGBGK_EINVAL (-1)    /* bad size, pointer or parameter */
+#define DGBGK_EMESH (-2)     /* inconsistent mesh (side or wall not found) */
+#define DGBGK_ECUDA (-3)     /* CUDA runtime error or no usable sm_100 GPU */
+#define DGBGK_ENONFINITE (-4) /* non-finite residual: the state diverged */
+#define DGBGK_EUNSUP (-5)    /* configuration not supported by this build */
+
+typedef struct dgbgk_handle dgbgk_handle;
+
+/* Mesh and the geometric arrays the reference computes during setup
+ * (src/dg_lin_convec.f90:96-125): GETSID, NORMAL, GETGEO, GETLEN,
+ * GETMAT/CONMAT, GETNOR.  dgbgk_setup_mesh() below computes them from
+ * INTMA, COORD and BSIDO the same way. */
+typedef struct dgbgk_mesh {
+  int nelem, npoin, nboun, nside;
+  const int* intma;     /* INTMA(3,NELEM)            src/gtinpt.f90:27-29  */
+  const double* coord;  /* COORD(2,NPOIN)            src/gtinpt.f90:36-38  */
+  const int* bsido;     /* BSIDO(6,NBOUN)            src/gtinpt.f90:48-50  */
+  const int* iside;     /* ISIDE(8,NSIDE)            src/getsid.f90:14-266 */
+  const double* nx;     /* NX(NSIDE)                 src/normal.f90:24-33  */
+  const double* ny;     /* NY(NSIDE)                                       */
+  const double* el;     /* EL(NSIDE)                                       */
+  const double* geome;  /* GEOME(7,NELEM)            src/getgeo.f90:22-59  */
+  const double* relen;  /* RELEN(NELEM)              src/getlen.f90:17-26  */
+  const double* mmat;   /* MMAT(3,NELEM), IMMAT = 1  src/getmat.f90:17-40  */
+  const double* cmmat;  /* CMMAT(3,3,NELEM), IMMAT=0 src/conmat.f90:17-41  */
+  const double* rsido;  /* RSIDO(3,NBOUN)            src/getnor.f90:21-31  */
+} dgbgk_mesh;
+
+/* Velocity space: VCORD(3,VNPNT) and SUMWEIGHT from VSPACE
+ * (src/vspace.f90:16-50); rv = IVD%rv. */
+typedef struct dgbgk_vspace {
+  int rorder, torder;
+  const double* vcord;
+  double sumweight;
+  double rv;
+} dgbgk_vspace;
+
+/* Physical and numerical parameters (the namelist of
+ * src/input_variable_module.f90:4-34 as ADVNCE receives them). */
+typedef struct dgbgk_params {
+  int immat;          /* 1: lumped mass (GETINC), 0: consistent (CMMINC)  */
+  double csafm;       /* Courant safety factor                            */
+  double alpha;       /* wall accommodation (1 = fully diffuse)           */
+  double rgas;        /* gas constant R                                   */
+  double molar_mass;  /* M                                                */
+  double diameter;    /* molecular diameter d                             */
+  double cinf[4];     /* inflow T, P [bar], U, V (zeros when IVD%INF = 0) */
+  /* Extensions: each reduces to the reference when left at its default.  */
+  int precision;      /* 64 (default): f in FP64; 32: f stored and swept
+                         in FP32 with FP64 moments and residual norms      */
+  const double* wall_velocity; /* (2,NBOUN) moving-wall velocity per
+                                  boundary side, or NULL (all at rest)    */
+  int tile_elems;     /* sweep tile: elements per CTA (0 = default)        */
+  int tile_vels;      /* sweep tile: velocities per CTA (0 = default)      */
+  int device;         /* CUDA device ordinal                               */
+} dgbgk_params;
+
+/* Fills a dgbgk_params with the reference defaults of
+ * src/spectralbgk.f90:116-147 plus precision 64. */
+void dgbgk_default_params(dgbgk_params* p);
+
+/* Host-side setup: GETSID (src/getsid.f90:14-266), NORMAL
+ * (src/normal.f90:24-33), GETGEO (src/getgeo.f90:22-59), GETLEN
+ * (src/getlen.f90:17-26), GETMAT (src/getmat.f90:17-40) or CONMAT
+ * (src/conmat.f90:17-41) and GETNOR (src/getnor.f90:21-31) from INTMA, COORD
+ * and BSIDO.  Output capacities: iside 8*mxsid, nx/ny/el mxsid with
+ * mxsid = 2*(nelem+nboun) (src/spectralbgk.f90:274); geome 7*nelem; relen
+ * nelem; mmat 3*nelem; cmmat 9*nelem; rsido 3*nboun.  *nside receives NSIDE. */
+int dgbgk_setup_mesh(int nelem, int npoin, int nboun, const int* intma, const double* coord,
+                     const int* bsido, int* nside, int* iside, double* nx, double* ny, double* el,
+                     double* geome, double* relen, double* mmat, double* cmmat, double* rsido);
+
+/* Velocity grid: VSPACE (src/vspace.f90:16-50) from the Lobatto pairs
+ * (eta_i, w_i), i = 1..rorder, with torder uniform angles.  vcord gets
+ * 3*rorder*torder values. */
+int dgbgk_vspace_build(int rorder, int torder, const double* eta, const double* w, double* vcord,
+                       double* sumweight);
+
+/* Creates a solver on the GPU; copies every input.  Replaces the setup part
+ * of ADVNCE (src/advnce.f90:127-148, ALOTIM and the first MACROS). */
+int dgbgk_create(const dgbgk_mesh* mesh, const dgbgk_vspace* vs, const dgbgk_params* prm,
+                 dgbgk_handle** out);
+
+/* State transfer in the reference layout DISNF(3,VNPNT,NELEM). */
+int dgbgk_set_state(dgbgk_handle* h, const double* disnf);
+int dgbgk_get_state(dgbgk_handle* h, double* disnf);
+int dgbgk_set_state_f32(dgbgk_handle* h, const float* disnf);
+int dgbgk_get_state_f32(dgbgk_handle* h, float* disnf);
+
+/* INICON2 (src/inicon2.f90:208-262): the uniform Maxwellian at T1, P1 [bar],
+ * (U0, V0), optionally scaled per DG node by node_scale(3,NELEM) (NULL = 1;
+ * the seeded density perturbation of the benchmark cases).  Built on the
+ * device. */
+int dgbgk_init_uniform(dgbgk_handle* h, double t1, double p1, double u0, double v0,
+                       const double* node_scale);
+
+/* Maxwellian per DG node from nodal fields (the warm start): number
+ * density n, velocity (u, v) and temperature T, each (3,NELEM) per DG node,
+ * with the INICON2 formula. */
+int dgbgk_init_maxwellian(dgbgk_handle* h, const double* n, const double* u, const double* v,
+                          const double* t);
+
+/* The ADVNCE time loop (src/advnce.f90:220-449): runs steps until max_steps
+ * have run or the L2 residual falls to tol_rel times the reference residual
+ * (tol_rel <= 0: run all max_steps).  The reference residual is the L2
+ * residual of the first step this handle ever ran unless set with
+ * dgbgk_set_residual_reference().  Per step, when non-NULL, res_linf gets
+ * max|DELUN| (the value behind RESIDUAL.RES, src/advnce.f90:422-429),
+ * res_l2 the L2 norm of DELUN and dte the time step.  *steps_done gets the
+ * number of steps run. */
+int dgbgk_advance(dgbgk_handle* h, int max_steps, double tol_rel, int* steps_done, double* res_linf,
+                  double* res_l2, double* dte);
+int dgbgk_set_residual_reference(dgbgk_handle* h, double res_l2_ref);
+int dgbgk_get_residual_reference(dgbgk_handle* h, double* res_l2_ref);
+
+/* MACROS (src/macros.f90:51-188) + GETMAC (src/getmac.f90:98-123) of the
+ * current state: nodal ND, RHO, UVEL, VVEL, PS, TEMP, NPOIN values each. */
+int dgbgk_get_macros(dgbgk_handle* h, double* nd, double* rho, double* u, double* v, double* ps,
+                     double* temp);
+
+/* Discontinuous per-DG-node fields of the current state (each (3,NELEM)):
+ * DISND, DISUX, DISUY, DISPS (src/macros.f90:131-164) and MU
+ * (src/compmu.f90:279-290).  Any pointer may be NULL. */
+int dgbgk_get_node_fields(dgbgk_handle* h, double* disnd, double* disux, double* disuy,
+                          double* disps, double* mu);
+
+/* FLUCON2 (src/flucon2.f90:43-241) of the current state: ETA(NBOUN). */
+int dgbgk_get_wall_eta(dgbgk_handle* h, double* eta);
+
+/* Sizes: [NELEM, NPOIN, NBOUN, NSIDE, VNPNT, precision, tile_elems,
+ * tile_vels, n_blocks, max_halo]. */
+int dgbgk_info(dgbgk_handle* h, int* out10);
+
+/* Device time of the last dgbgk_advance() call in ms (CUDA events on the
+ * library's stream around the whole time loop). */
+int dgbgk_last_timing(dgbgk_handle* h, double* total_ms);
+
+/* Runs nsteps time steps launch by launch (no graph) with CUDA events
+ * between the kernels on the library's stream; kernel_ms[4] receives the
+ * mean device time per step of [moments, wall flux, sweep, residual]. The
+ * state advances by nsteps steps exactly as under dgbgk_advance(). */
+int dgbgk_profile_steps(dgbgk_handle* h, int nsteps, double* kernel_ms);
+
+void dgbgk_destroy(dgbgk_handle* h);
+const char* dgbgk_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DGBGK_H */

@@ -1,0 +1,49 @@
+"""The C-ABI library loads and exports every entry point include/dgbgk.h
+declares; without a GPU it refuses to run instead of falling back (CPU)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from conftest import ROOT
+
+
+def declared():
+    src = open(os.path.join(ROOT, "include", "dgbgk.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(dgbgk_\w+)\s*\(", src)))
+
+
+def test_header_declares_the_abi():
+    names = declared()
+    for n in ("dgbgk_create", "dgbgk_advance", "dgbgk_set_state", "dgbgk_get_state", "dgbgk_get_macros",
+              "dgbgk_destroy", "dgbgk_last_error", "dgbgk_setup_mesh"):
+        assert n in names
+
+
+def test_library_exports_every_declared_symbol():
+    from dgbgk import _lib
+    L = ctypes.CDLL(_lib.LIB_PATH)
+    missing = [n for n in declared() if not hasattr(L, n)]
+    assert not missing, missing
+    # the Python binding covers the same set
+    assert set(declared()) <= set(_lib.SIGNATURES)
+
+
+def _has_gpu():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+@pytest.mark.skipif(_has_gpu(), reason="checks the no-GPU failure path")
+def test_create_without_gpu_fails_loudly():
+    from dgbgk import cavity_case, Solver
+    from dgbgk._lib import DgbgkError, DGBGK_ECUDA
+    with pytest.raises(DgbgkError) as ei:
+        Solver.from_case(cavity_case(4, 4, 8))
+    assert ei.value.code == DGBGK_ECUDA
+    assert "no CPU fallback" in str(ei.value) or "CUDA" in str(ei.value)

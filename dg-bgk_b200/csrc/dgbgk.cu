@@ -1,6 +1,9 @@
 // C ABI of the DG-BGK sweep on B200 (sm_100a): handle management, device
-// memory, the captured two-step CUDA graph and the state transfers.
+// memory, TMA descriptors, the captured two-step CUDA graph and the state
+// transfers.
+#include <cuda.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <cmath>
@@ -49,6 +52,22 @@ template <class X> int upload(X** p, const std::vector<X>& v, cudaStream_t s) {
   if (!v.empty()) CK(cudaMemcpyAsync(*p, v.data(), v.size() * sizeof(X), cudaMemcpyHostToDevice, s));
   return 0;
 }
+template <class X> void dfree(X*& p) {
+  if (p) cudaFree((void*)p);
+  p = nullptr;
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    cudaDriverEntryPointQueryResult q;
+    void* p = nullptr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+  }
+  return fn;
+}
 
 struct ImplBase {
   virtual ~ImplBase() {}
@@ -65,23 +84,26 @@ struct ImplBase {
   Plan pl;
   int device = 0;
   int prec = 64;
+  int nsm = 148;
   double ref_host = 0.0;
   float last_ms = 0.f;
 };
 
 template <class T> struct Impl : ImplBase {
+  static constexpr int TY = 8;  // warps per sweep CTA
   cudaStream_t st = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, evpoll[2] = {nullptr, nullptr};
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
   int cur = 0;
-  int M = 4, TY = 8, VT = 32;
+  int M = 4;
+  int Vp = 0;
   // device arrays
   T* f[2] = {nullptr, nullptr};
-  ElemGeo<T>* geo = nullptr;
-  ElemEdge<T>* edge = nullptr;
-  int *eslot = nullptr, *halo_off = nullptr, *halo_list = nullptr;
+  CUtensorMap tm_blk[2], tm_row3[2];
+  ElemRec<T>* rec = nullptr;
+  int *halo_off = nullptr, *halo_list = nullptr;
   T *cmax = nullptr, *cmin = nullptr;
-  NodeP<T>* np = nullptr;
+  T* tabs = nullptr;  // moment tables [3][Vp]
   double *nraw = nullptr, *disux = nullptr, *disuy = nullptr, *disps = nullptr, *mu = nullptr;
   T *cxT = nullptr, *cyT = nullptr, *nfT = nullptr;
   double *cxD = nullptr, *cyD = nullptr, *wjf = nullptr;
@@ -91,26 +113,56 @@ template <class T> struct Impl : ImplBase {
   int *node_off = nullptr, *node_dg = nullptr;
   double* node_ae = nullptr;
   double *part_max = nullptr, *part_sq = nullptr;
-  int nparts = 0;
+  int nparts = 0, sweep_grid = 0, part_cap = 0;
+  int mom_grid = 0, mom_warps = 0, mom_stages = 0;
+  size_t mom_smem = 0;
   double *hist_linf = nullptr, *hist_l2 = nullptr, *hist_dt = nullptr;
   int hist_cap = 0;
   Ctrl* ctrl = nullptr;
   Ctrl* hctrl = nullptr;  // pinned: [0] upload, [1..2] polls
   void* staging = nullptr;
   size_t staging_bytes = 0;
+  int* d_inv = nullptr;
 
   ~Impl() override {
     cudaSetDevice(device);
     if (st) cudaStreamSynchronize(st);
     drop_graphs();
-    if (d_inv) cudaFree(d_inv);
-    void* ptrs[] = {f[0],     f[1],      geo,     edge,     eslot,    halo_off, halo_list, cmax,
-                    cmin,     np,        nraw,    disux,    disuy,    disps,    mu,        cxT,
-                    cyT,      nfT,       cxD,     cyD,      wjf,      bTw,      bUw,       bEta,
-                    bEtaD,    walls,     node_off, node_dg, node_ae, part_max, part_sq,   hist_linf,
-                    hist_l2,  hist_dt,   ctrl,    staging};
-    for (void* p : ptrs)
-      if (p) cudaFree(p);
+    dfree(d_inv);
+    dfree(f[0]);
+    dfree(f[1]);
+    dfree(rec);
+    dfree(tabs);
+    dfree(halo_off);
+    dfree(halo_list);
+    dfree(cmax);
+    dfree(cmin);
+    dfree(nraw);
+    dfree(disux);
+    dfree(disuy);
+    dfree(disps);
+    dfree(mu);
+    dfree(cxT);
+    dfree(cyT);
+    dfree(nfT);
+    dfree(cxD);
+    dfree(cyD);
+    dfree(wjf);
+    dfree(bTw);
+    dfree(bUw);
+    dfree(bEta);
+    dfree(bEtaD);
+    dfree(walls);
+    dfree(node_off);
+    dfree(node_dg);
+    dfree(node_ae);
+    dfree(part_max);
+    dfree(part_sq);
+    dfree(hist_linf);
+    dfree(hist_l2);
+    dfree(hist_dt);
+    dfree(ctrl);
+    if (staging) cudaFree(staging);
     if (hctrl) cudaFreeHost(hctrl);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
@@ -119,45 +171,27 @@ template <class T> struct Impl : ImplBase {
     if (st) cudaStreamDestroy(st);
   }
 
-  int ntiles() const { return (pl.V + VT - 1) / VT; }
-  size_t sweep_smem() const { return (size_t)(pl.EB + pl.max_halo) * 4 * VT * sizeof(T); }
+  int nvt() const { return (pl.V + VTILE - 1) / VTILE; }
+  static int default_m() { return sizeof(T) == 8 ? 3 : 6; }
+  int slots() const { return pl.EB + pl.max_halo; }
+  size_t sweep_smem() const { return SweepSmem<T>(pl.EB, slots()).total; }
 
   int init(int tile_elems) {
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
     CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     CK(cudaEventCreate(&ev0));
     CK(cudaEventCreate(&ev1));
     for (auto& e : evpoll) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-    const size_t n = (size_t)3 * pl.E * pl.V;
+    Vp = ((pl.V + 31) / 32) * 32;
+    const size_t n = (size_t)3 * pl.E * Vp;
     TRY(dalloc(&f[0], n));
     TRY(dalloc(&f[1], n));
     CK(cudaMemsetAsync(f[0], 0, n * sizeof(T), st));
-    std::vector<ElemGeo<T>> g(pl.E);
-    for (int e = 0; e < pl.E; ++e) {
-      const auto& s = pl.geo[e];
-      for (int k = 0; k < 3; ++k) {
-        g[e].gx[k] = (T)s.gx[k];
-        g[e].gy[k] = (T)s.gy[k];
-        g[e].mm[k] = (T)s.mm[k];
-      }
-      g[e].area = (T)s.area;
-      g[e].inflow = s.inflow;
-      g[e].pad = 0;
-    }
-    TRY(upload(&geo, g, st));
-    std::vector<ElemEdge<T>> ed(pl.edge.size());
-    for (size_t i = 0; i < ed.size(); ++i) {
-      ed[i].nx = (T)pl.edge[i].nx;
-      ed[i].ny = (T)pl.edge[i].ny;
-      ed[i].alen = (T)pl.edge[i].alen;
-      ed[i].nbr = pl.edge[i].nbr;
-      ed[i].info = pl.edge[i].info;
-    }
-    TRY(upload(&edge, ed, st));
+    CK(cudaMemsetAsync(f[1], 0, n * sizeof(T), st));
     std::vector<T> cm(pl.cmax.begin(), pl.cmax.end()), cn(pl.cmin.begin(), pl.cmin.end());
     TRY(upload(&cmax, cm, st));
     TRY(upload(&cmin, cn, st));
     const size_t ndg = 3 * (size_t)pl.E;
-    TRY(dalloc(&np, ndg));
     TRY(dalloc(&nraw, ndg));
     TRY(dalloc(&disux, ndg));
     TRY(dalloc(&disuy, ndg));
@@ -171,6 +205,13 @@ template <class T> struct Impl : ImplBase {
     TRY(upload(&cxD, pl.cx, st));
     TRY(upload(&cyD, pl.cy, st));
     TRY(upload(&wjf, pl.wjf, st));
+    std::vector<T> tb(3 * (size_t)Vp, (T)0);  // zero past V
+    for (int v = 0; v < pl.V; ++v) {
+      tb[v] = (T)pl.cx[v];
+      tb[Vp + v] = (T)pl.cy[v];
+      tb[2 * (size_t)Vp + v] = (T)pl.wjf[v];
+    }
+    TRY(upload(&tabs, tb, st));
     std::vector<T> tw(pl.bTw.begin(), pl.bTw.end()), uw(pl.bUw.begin(), pl.bUw.end()),
         z(std::max(pl.B, 1), (T)0);
     TRY(upload(&bTw, tw, st));
@@ -186,53 +227,153 @@ template <class T> struct Impl : ImplBase {
     CK(cudaMallocHost((void**)&hctrl, 3 * sizeof(Ctrl)));
     std::memset(hctrl, 0, 3 * sizeof(Ctrl));
     CK(cudaMemcpyAsync(ctrl, hctrl, sizeof(Ctrl), cudaMemcpyHostToDevice, st));
+    TRY(config_moments());
     TRY(set_tile(tile_elems));
     TRY(ensure_hist(1024));
     CK(cudaStreamSynchronize(st));
     return 0;
   }
 
-  // Sweep tile: elements per CTA = TY*M with TY = 8 rows of VT = 32 lanes.
+  // Moment kernel: per-warp rings of velocity rows, persistent grid.  Picks
+  // the (warps per CTA, ring stages) with the most resident warps per SM.
+  int config_moments() {
+    const size_t rowbytes = ((size_t)pl.V * sizeof(T) + 15) / 16 * 16;
+    const size_t tbytes = 3 * (size_t)Vp * sizeof(T);
+    const size_t cap = 227 * 1024, sm_total = 228 * 1024;
+    int best = -1;
+    for (int w : {16, 12, 8, 6, 4, 2, 1})
+      for (int sg : {3, 2}) {
+        const size_t bytes = 128 * (((size_t)w * sg * 8 + 127) / 128) + tbytes + (size_t)w * sg * rowbytes;
+        if (bytes > cap) continue;
+        const int blocks = (int)std::min<size_t>(4, sm_total / (bytes + 1024));
+        const int score = blocks * w * 4 + sg;  // resident warps first, then stages
+        if (blocks >= 1 && score > best) {
+          best = score;
+          mom_warps = w;
+          mom_stages = sg;
+          mom_smem = bytes;
+        }
+      }
+    if (best < 0) {
+      set_error("velocity rows too long for the moment kernel's shared-memory ring");
+      return DGBGK_EUNSUP;
+    }
+    const int warps = mom_warps;
+    CK(cudaFuncSetAttribute(k_moments<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mom_smem));
+    int per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_moments<T>, warps * 32, mom_smem));
+    if (per_sm < 1) per_sm = 1;
+    const int ndg = 3 * pl.E;
+    const int need = (ndg + warps - 1) / warps;
+    mom_grid = std::max(1, std::min(need, per_sm * nsm));
+    return 0;
+  }
+
+  template <int MM> int sweep_occupancy(int* per_sm) {
+    CK(cudaFuncSetAttribute(k_sweep<T, MM, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sweep_smem()));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_sweep<T, MM, TY>, 32 * TY, sweep_smem()));
+    return 0;
+  }
+
+  int make_tensor_maps() {
+    auto enc = tensor_map_encoder();
+    if (!enc) {
+      set_error("cuTensorMapEncodeTiled is not available from the driver");
+      return DGBGK_ECUDA;
+    }
+    const CUtensorMapDataType dt = sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    cuuint64_t dims[2] = {(cuuint64_t)pl.V, (cuuint64_t)3 * pl.E};
+    cuuint64_t strides[1] = {(cuuint64_t)Vp * sizeof(T)};
+    cuuint32_t estr[2] = {1, 1};
+    for (int b = 0; b < 2; ++b) {
+      cuuint32_t box_blk[2] = {(cuuint32_t)VTILE, (cuuint32_t)(3 * pl.EB)};
+      cuuint32_t box_row[2] = {(cuuint32_t)VTILE, 3u};
+      CUresult r1 = enc(&tm_blk[b], dt, 2, f[b], dims, strides, box_blk, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                        CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      CUresult r2 = enc(&tm_row3[b], dt, 2, f[b], dims, strides, box_row, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                        CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      if (r1 != CUDA_SUCCESS || r2 != CUDA_SUCCESS) {
+        set_error("cuTensorMapEncodeTiled failed for the state buffer");
+        return DGBGK_ECUDA;
+      }
+    }
+    return 0;
+  }
+
+  // Sweep tile: elements per CTA = 8 warps x M elements per warp.
   int set_tile(int tile_elems) {
-    int m = tile_elems > 0 ? tile_elems / 8 : (sizeof(T) == 8 ? 4 : 8);
-    if (m != 1 && m != 2 && m != 4 && m != 8) {
-      set_error("tile_elems must be 8, 16, 32 or 64");
+    const int m = tile_elems > 0 ? tile_elems / TY : default_m();
+    if ((m != 2 && m != 3 && m != 4 && m != 6 && m != 8) || (tile_elems > 0 && tile_elems % TY)) {
+      set_error("tile_elems must be 16, 24, 32, 48 or 64");
       return DGBGK_EINVAL;
     }
     M = m;
-    TY = 8;
-    VT = 32;
     if (pl.EB != TY * M || halo_off == nullptr) {
       build_blocks(pl, TY * M);
-      if (halo_off) cudaFree(halo_off);
-      if (halo_list) cudaFree(halo_list);
-      if (eslot) cudaFree(eslot);
+      dfree(halo_off);
+      dfree(halo_list);
+      dfree(rec);
       TRY(upload(&halo_off, pl.halo_off, st));
       TRY(upload(&halo_list, pl.halo_list, st));
-      TRY(upload(&eslot, pl.eslot, st));
+      // element records: geometry, mass matrix and edges (the node
+      // parameters are filled by the moment kernel before every sweep)
+      std::vector<ElemRec<T>> r(pl.E);
+      std::memset((void*)r.data(), 0, r.size() * sizeof(ElemRec<T>));
+      for (int e = 0; e < pl.E; ++e) {
+        const auto& g = pl.geo[e];
+        for (int k = 0; k < 3; ++k) {
+          r[e].gx[k] = (T)g.gx[k];
+          r[e].gy[k] = (T)g.gy[k];
+          r[e].mm[k] = (T)g.mm[k];
+          const size_t i = 3 * (size_t)e + k;
+          r[e].edge[k].nx = (T)pl.edge[i].nx;
+          r[e].edge[k].ny = (T)pl.edge[i].ny;
+          r[e].edge[k].alen = (T)pl.edge[i].alen;
+          r[e].edge[k].info = edge_info(pl, i);
+        }
+        r[e].area = (T)g.area;
+        r[e].inflow = g.inflow;
+      }
+      TRY(upload(&rec, r, st));
     }
     if (sweep_smem() > 227 * 1024) {
       set_error("sweep tile needs more than 227 KB of shared memory");
       return DGBGK_EUNSUP;
     }
-    const int np_ = pl.nblocks * ntiles();
-    if (np_ > nparts) {
-      if (part_max) cudaFree(part_max);
-      if (part_sq) cudaFree(part_sq);
-      TRY(dalloc(&part_max, np_));
-      TRY(dalloc(&part_sq, np_));
+    TRY(make_tensor_maps());
+    int per_sm = 0;
+    switch (M) {
+      case 2: TRY(sweep_occupancy<2>(&per_sm)); break;
+      case 3: TRY(sweep_occupancy<3>(&per_sm)); break;
+      case 4: TRY(sweep_occupancy<4>(&per_sm)); break;
+      case 6: TRY(sweep_occupancy<6>(&per_sm)); break;
+      default: TRY(sweep_occupancy<8>(&per_sm)); break;
     }
-    nparts = np_;
+    if (per_sm < 1) {
+      set_error("sweep kernel does not fit on an SM with this tile");
+      return DGBGK_EUNSUP;
+    }
+    const int ntiles = pl.nblocks * nvt();
+    sweep_grid = std::max(1, std::min(ntiles, per_sm * nsm));
+    if (sweep_grid > part_cap) {
+      dfree(part_max);
+      dfree(part_sq);
+      TRY(dalloc(&part_max, sweep_grid));
+      TRY(dalloc(&part_sq, sweep_grid));
+      part_cap = sweep_grid;
+    }
+    nparts = sweep_grid;
     drop_graphs();
-    attrs_primed = false;
     return 0;
   }
 
   int ensure_hist(int n) {
     if (n <= hist_cap) return 0;
-    if (hist_linf) cudaFree(hist_linf);
-    if (hist_l2) cudaFree(hist_l2);
-    if (hist_dt) cudaFree(hist_dt);
+    dfree(hist_linf);
+    dfree(hist_l2);
+    dfree(hist_dt);
     TRY(dalloc(&hist_linf, n));
     TRY(dalloc(&hist_l2, n));
     TRY(dalloc(&hist_dt, n));
@@ -242,31 +383,40 @@ template <class T> struct Impl : ImplBase {
   }
 
   // -------------------------------------------------------- launches ----
-  int launch_moments(const T* src) {
-    constexpr int WPB = 4;
-    MomArgs<T> a{src, cxD, cyD, wjf, np, nraw, disux, disuy, disps, mu, ctrl, 3 * pl.E, pl.V,
-                 pl.M / 6.022e26, 3.1416 * pl.d * pl.d};
-    const size_t smem = (size_t)WPB * pl.V * sizeof(T);
+  int launch_moments(int src) {
+    MomArgs<T> a;
+    a.f = f[src];
+    a.tabs = tabs;
+    a.rec = rec;
+    a.nraw = nraw;
+    a.disux = disux;
+    a.disuy = disuy;
+    a.disps = disps;
+    a.mu = mu;
+    a.ctrl = ctrl;
+    a.ndg = 3 * pl.E;
+    a.V = pl.V;
+    a.Vp = Vp;
+    a.nstage = mom_stages;
+    a.rowbytes = (unsigned)(((size_t)pl.V * sizeof(T) + 15) / 16 * 16);
+    a.MM = pl.M / 6.022e26;
+    a.sigt = 3.1416 * pl.d * pl.d;
     CK(cudaMemsetAsync(&ctrl->maxmu, 0, sizeof(double), st));
-    k_moments<T, WPB><<<(a.ndg + WPB - 1) / WPB, WPB * 32, smem, st>>>(a);
+    k_moments<T><<<mom_grid, mom_warps * 32, mom_smem, st>>>(a);
     CK(cudaGetLastError());
     return 0;
   }
-  int launch_wall(const T* src) {
+  int launch_wall(int src) {
     if (pl.walls.empty()) return 0;
-    WallArgs<T> a{src, walls, cxD, cyD, wjf, bEta, bEtaD, ctrl, (int)pl.walls.size(), pl.V};
+    WallArgs<T> a{f[src], walls, cxD, cyD, wjf, bEta, bEtaD, ctrl, (int)pl.walls.size(), pl.V, Vp};
     k_wall<T><<<(a.nwall + 7) / 8, 256, 0, st>>>(a);
     CK(cudaGetLastError());
     return 0;
   }
-  int launch_sweep(const T* src, T* dst) {
+  int launch_sweep(int src) {
     SweepArgs<T> a;
-    a.fin = src;
-    a.fout = dst;
-    a.geo = geo;
-    a.edge = edge;
-    a.eslot = eslot;
-    a.np = np;
+    a.fout = f[1 - src];
+    a.rec = rec;
     a.halo_off = halo_off;
     a.halo_list = halo_list;
     a.cx = cxT;
@@ -282,24 +432,23 @@ template <class T> struct Impl : ImplBase {
     a.ctrl = ctrl;
     a.E = pl.E;
     a.V = pl.V;
+    a.Vp = Vp;
     a.EB = pl.EB;
-    a.slots = pl.EB + pl.max_halo;
+    a.slots = slots();
+    a.nblocks = pl.nblocks;
+    a.nvt = nvt();
     a.immat = pl.immat;
     a.alpha = (T)pl.alpha;
     a.rgas = (T)pl.rgas;
-    dim3 grid(pl.nblocks, ntiles()), block(VT, TY);
+    const dim3 block(32, TY);
     const size_t smem = sweep_smem();
-#define DGBGK_SWEEP(MM)                         \
-  case MM:                                      \
-    k_sweep<T, MM><<<grid, block, smem, st>>>(a); \
-    break;
     switch (M) {
-      DGBGK_SWEEP(1)
-      DGBGK_SWEEP(2)
-      DGBGK_SWEEP(4)
-      DGBGK_SWEEP(8)
+      case 2: k_sweep<T, 2, TY><<<sweep_grid, block, smem, st>>>(tm_blk[src], tm_row3[src], a); break;
+      case 3: k_sweep<T, 3, TY><<<sweep_grid, block, smem, st>>>(tm_blk[src], tm_row3[src], a); break;
+      case 4: k_sweep<T, 4, TY><<<sweep_grid, block, smem, st>>>(tm_blk[src], tm_row3[src], a); break;
+      case 6: k_sweep<T, 6, TY><<<sweep_grid, block, smem, st>>>(tm_blk[src], tm_row3[src], a); break;
+      default: k_sweep<T, 8, TY><<<sweep_grid, block, smem, st>>>(tm_blk[src], tm_row3[src], a); break;
     }
-#undef DGBGK_SWEEP
     CK(cudaGetLastError());
     return 0;
   }
@@ -310,9 +459,9 @@ template <class T> struct Impl : ImplBase {
     return 0;
   }
   int enqueue_step(int src) {
-    TRY(launch_moments(f[src]));
-    TRY(launch_wall(f[src]));
-    TRY(launch_sweep(f[src], f[1 - src]));
+    TRY(launch_moments(src));
+    TRY(launch_wall(src));
+    TRY(launch_sweep(src));
     TRY(launch_resid());
     return 0;
   }
@@ -328,8 +477,6 @@ template <class T> struct Impl : ImplBase {
   int build_graph(int s) {
     if (gexec[s]) return 0;
     cudaGraph_t g;
-    // attribute calls are not stream work: done once, before capture
-    TRY(prime_attributes());
     CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     int rc = enqueue_step(s);
     if (rc == 0) rc = enqueue_step(1 - s);
@@ -340,33 +487,28 @@ template <class T> struct Impl : ImplBase {
     cudaGraphDestroy(g);
     return 0;
   }
-  bool attrs_primed = false;
-  int prime_attributes() {
-    if (attrs_primed) return 0;
-    constexpr int WPB = 4;
-    CK(cudaFuncSetAttribute(k_moments<T, WPB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)((size_t)WPB * pl.V * sizeof(T))));
-    const int smem = (int)sweep_smem();
-    CK(cudaFuncSetAttribute(k_sweep<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    CK(cudaFuncSetAttribute(k_sweep<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    CK(cudaFuncSetAttribute(k_sweep<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    CK(cudaFuncSetAttribute(k_sweep<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    attrs_primed = true;
-    return 0;
-  }
 
   int upload_ctrl(int max_steps, double tol) {
     Ctrl& h = hctrl[0];
     std::memset(&h, 0, sizeof(Ctrl));
-    h.done = 0;
-    h.step = 0;
     h.max_steps = max_steps;
     h.tol = tol;
     h.ref = ref_host;
-    h.maxmu = 0;
     h.dtc = pl.dtc;
     h.nparts = nparts;
     CK(cudaMemcpyAsync(ctrl, &h, sizeof(Ctrl), cudaMemcpyHostToDevice, st));
+    return 0;
+  }
+
+  int finish_status(const Ctrl& c) {
+    if (c.timeout) {
+      set_error("a bounded device wait expired (asynchronous copy did not complete)");
+      return DGBGK_ECUDA;
+    }
+    if (c.nonfinite) {
+      set_error("non-finite residual: the state diverged");
+      return DGBGK_ENONFINITE;
+    }
     return 0;
   }
 
@@ -378,7 +520,6 @@ template <class T> struct Impl : ImplBase {
     if (steps) *steps = 0;
     if (max_steps == 0) return 0;
     CK(cudaSetDevice(device));
-    if (prime_attributes()) return DGBGK_ECUDA;
     TRY(ensure_hist(max_steps));
     const int s0 = cur;
     TRY(build_graph(s0));
@@ -406,7 +547,7 @@ template <class T> struct Impl : ImplBase {
     CK(cudaMemcpyAsync(&hctrl[1], ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     CK(cudaEventElapsedTime(&last_ms, ev0, ev1));
-    const Ctrl& c = hctrl[1];
+    const Ctrl c = hctrl[1];
     const int ns = c.step;
     if (steps) *steps = ns;
     ref_host = c.ref;
@@ -416,18 +557,45 @@ template <class T> struct Impl : ImplBase {
       if (dt) CK(cudaMemcpy(dt, hist_dt, ns * sizeof(double), cudaMemcpyDeviceToHost));
     }
     cur = s0 ^ (ns & 1);
-    if (c.nonfinite) {
-      set_error("non-finite residual: the state diverged");
-      return DGBGK_ENONFINITE;
-    }
-    return 0;
+    return finish_status(c);
   }
 
-  // aux kernels run with done = 0
-  int aux_ctrl() {
-    TRY(upload_ctrl(1, 0.0));
-    return 0;
+  int profile(int nsteps, double* ms) override {
+    CK(cudaSetDevice(device));
+    TRY(ensure_hist(std::max(nsteps, 1)));
+    TRY(upload_ctrl(nsteps, 0.0));
+    cudaEvent_t ev[5];
+    for (auto& e : ev) CK(cudaEventCreate(&e));
+    double acc[4] = {0, 0, 0, 0};
+    int rc = 0;
+    for (int s = 0; s < nsteps && rc == 0; ++s) {
+      cudaEventRecord(ev[0], st);
+      rc = launch_moments(cur);
+      cudaEventRecord(ev[1], st);
+      if (rc == 0) rc = launch_wall(cur);
+      cudaEventRecord(ev[2], st);
+      if (rc == 0) rc = launch_sweep(cur);
+      cudaEventRecord(ev[3], st);
+      if (rc == 0) rc = launch_resid();
+      cudaEventRecord(ev[4], st);
+      cudaEventSynchronize(ev[4]);
+      for (int k = 0; k < 4; ++k) {
+        float t = 0;
+        cudaEventElapsedTime(&t, ev[k], ev[k + 1]);
+        acc[k] += t;
+      }
+      cur ^= 1;
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    if (rc) return rc;
+    CK(cudaMemcpy(&hctrl[1], ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost));
+    ref_host = hctrl[1].ref;
+    for (int k = 0; k < 4; ++k) ms[k] = nsteps > 0 ? acc[k] / nsteps : 0.0;
+    return finish_status(hctrl[1]);
   }
+
+  // auxiliary kernels run with done = 0
+  int aux_ctrl() { return upload_ctrl(1, 0.0); }
 
   int set_state(const void* src, bool f32) override {
     CK(cudaSetDevice(device));
@@ -437,9 +605,9 @@ template <class T> struct Impl : ImplBase {
     CK(cudaMemcpyAsync(staging, src, bytes, cudaMemcpyHostToDevice, st));
     TRY(upload_perm());
     if (f32)
-      k_to_internal<float, T><<<pl.E, 256, 0, st>>>((const float*)staging, f[0], d_inv, pl.V);
+      k_to_internal<float, T><<<pl.E, 256, 0, st>>>((const float*)staging, f[0], d_inv, pl.V, Vp);
     else
-      k_to_internal<double, T><<<pl.E, 256, 0, st>>>((const double*)staging, f[0], d_inv, pl.V);
+      k_to_internal<double, T><<<pl.E, 256, 0, st>>>((const double*)staging, f[0], d_inv, pl.V, Vp);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(st));
     cur = 0;
@@ -452,15 +620,14 @@ template <class T> struct Impl : ImplBase {
     TRY(ensure_staging(bytes));
     TRY(upload_perm());
     if (f32)
-      k_from_internal<T, float><<<pl.E, 256, 0, st>>>(f[cur], (float*)staging, d_inv, pl.V);
+      k_from_internal<T, float><<<pl.E, 256, 0, st>>>(f[cur], (float*)staging, d_inv, pl.V, Vp);
     else
-      k_from_internal<T, double><<<pl.E, 256, 0, st>>>(f[cur], (double*)staging, d_inv, pl.V);
+      k_from_internal<T, double><<<pl.E, 256, 0, st>>>(f[cur], (double*)staging, d_inv, pl.V, Vp);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(dst, staging, bytes, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     return 0;
   }
-  int* d_inv = nullptr;
   int upload_perm() {
     if (d_inv) return 0;
     TRY(upload(&d_inv, pl.inv, st));
@@ -470,6 +637,7 @@ template <class T> struct Impl : ImplBase {
     if (bytes <= staging_bytes) return 0;
     if (staging) cudaFree(staging);
     staging = nullptr;
+    staging_bytes = 0;
     CK(cudaMalloc(&staging, bytes));
     staging_bytes = bytes;
     return 0;
@@ -504,9 +672,8 @@ template <class T> struct Impl : ImplBase {
     double *dg = nullptr, *dsc = nullptr;
     TRY(upload(&dg, g, st));
     if (scale) TRY(upload(&dsc, sc, st));
-    const size_t total = (size_t)3 * pl.E * pl.V;
-    k_init_uniform<T><<<(unsigned)((total + 255) / 256), 256, 0, st>>>(f[0], dg, dsc, vacuum ? 0.0 : n1, pl.V,
-                                                                       total);
+    const size_t ndg = (size_t)3 * pl.E;
+    k_init_uniform<T><<<(unsigned)ndg, 128, 0, st>>>(f[0], dg, dsc, vacuum ? 0.0 : n1, pl.V, Vp, ndg);
     cudaError_t e = cudaGetLastError();
     cudaStreamSynchronize(st);
     cudaFree(dg);
@@ -529,9 +696,9 @@ template <class T> struct Impl : ImplBase {
       }
     double* dp = nullptr;
     TRY(upload(&dp, prm, st));
-    const size_t total = (size_t)3 * pl.E * pl.V;
-    k_init_maxwellian<T><<<(unsigned)((total + 255) / 256), 256, 0, st>>>(f[0], dp, cxD, cyD, pl.M / 6.022e26,
-                                                                          pl.rgas, pl.V, total);
+    const size_t ndg = (size_t)3 * pl.E;
+    k_init_maxwellian<T><<<(unsigned)ndg, 128, 0, st>>>(f[0], dp, cxD, cyD, pl.M / 6.022e26, pl.rgas, pl.V, Vp,
+                                                         ndg);
     cudaError_t e = cudaGetLastError();
     cudaStreamSynchronize(st);
     cudaFree(dp);
@@ -541,9 +708,8 @@ template <class T> struct Impl : ImplBase {
   }
 
   int moments_now() {
-    TRY(prime_attributes());
     TRY(aux_ctrl());
-    TRY(launch_moments(f[cur]));
+    TRY(launch_moments(cur));
     return 0;
   }
 
@@ -562,6 +728,8 @@ template <class T> struct Impl : ImplBase {
     cudaStreamSynchronize(st);
     cudaFree(out);
     CK(e);
+    CK(cudaMemcpy(&hctrl[1], ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost));
+    TRY(finish_status(hctrl[1]));
     double* dsts[6] = {nd, rho, u, v, ps, temp};
     for (int k = 0; k < 6; ++k)
       if (dsts[k]) std::memcpy(dsts[k], h.data() + (size_t)k * pl.NP, pl.NP * sizeof(double));
@@ -579,6 +747,8 @@ template <class T> struct Impl : ImplBase {
     CK(cudaMemcpyAsync(h.data() + 3 * ndg, disps, ndg * 8, cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(h.data() + 4 * ndg, mu, ndg * 8, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    CK(cudaMemcpy(&hctrl[1], ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost));
+    TRY(finish_status(hctrl[1]));
     double* dsts[5] = {nd, ux, uy, ps, muo};
     for (int k = 0; k < 5; ++k) {
       if (!dsts[k]) continue;
@@ -596,48 +766,9 @@ template <class T> struct Impl : ImplBase {
     CK(cudaSetDevice(device));
     TRY(aux_ctrl());
     CK(cudaMemsetAsync(bEtaD, 0, std::max(pl.B, 1) * sizeof(double), st));
-    TRY(launch_wall(f[cur]));
-    CK(cudaMemcpyAsync(eta, bEtaD, pl.B * sizeof(double), cudaMemcpyDeviceToHost, st));
+    TRY(launch_wall(cur));
+    if (pl.B) CK(cudaMemcpyAsync(eta, bEtaD, pl.B * sizeof(double), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
-    return 0;
-  }
-
-  int profile(int nsteps, double* ms) override {
-    CK(cudaSetDevice(device));
-    TRY(prime_attributes());
-    TRY(ensure_hist(std::max(nsteps, 1)));
-    TRY(upload_ctrl(nsteps, 0.0));
-    cudaEvent_t ev[5];
-    for (auto& e : ev) CK(cudaEventCreate(&e));
-    double acc[4] = {0, 0, 0, 0};
-    int rc = 0;
-    for (int s = 0; s < nsteps && rc == 0; ++s) {
-      cudaEventRecord(ev[0], st);
-      rc = launch_moments(f[cur]);
-      cudaEventRecord(ev[1], st);
-      if (rc == 0) rc = launch_wall(f[cur]);
-      cudaEventRecord(ev[2], st);
-      if (rc == 0) rc = launch_sweep(f[cur], f[1 - cur]);
-      cudaEventRecord(ev[3], st);
-      if (rc == 0) rc = launch_resid();
-      cudaEventRecord(ev[4], st);
-      cudaEventSynchronize(ev[4]);
-      for (int k = 0; k < 4; ++k) {
-        float t = 0;
-        cudaEventElapsedTime(&t, ev[k], ev[k + 1]);
-        acc[k] += t;
-      }
-      cur ^= 1;
-    }
-    for (auto& e : ev) cudaEventDestroy(e);
-    if (rc) return rc;
-    CK(cudaMemcpy(&hctrl[1], ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost));
-    ref_host = hctrl[1].ref;
-    for (int k = 0; k < 4; ++k) ms[k] = nsteps > 0 ? acc[k] / nsteps : 0.0;
-    if (hctrl[1].nonfinite) {
-      set_error("non-finite residual: the state diverged");
-      return DGBGK_ENONFINITE;
-    }
     return 0;
   }
 
@@ -649,7 +780,7 @@ template <class T> struct Impl : ImplBase {
     o[4] = pl.V;
     o[5] = prec;
     o[6] = pl.EB;
-    o[7] = VT;
+    o[7] = VTILE;
     o[8] = pl.nblocks;
     o[9] = pl.max_halo;
   }
@@ -702,7 +833,7 @@ int dgbgk_create(const dgbgk_mesh* mesh, const dgbgk_vspace* vs, const dgbgk_par
   impl->device = prm->device;
   impl->prec = prm->precision;
   std::string err;
-  const int eb0 = prm->tile_elems > 0 ? prm->tile_elems : (prm->precision == 64 ? 32 : 64);
+  const int eb0 = prm->tile_elems > 0 ? prm->tile_elems : (prm->precision == 64 ? 24 : 48);
   int rc = build_plan(*mesh, *vs, *prm, eb0, impl->pl, &err);
   if (rc != 0) {
     set_error(err);
@@ -721,12 +852,12 @@ int dgbgk_create(const dgbgk_mesh* mesh, const dgbgk_vspace* vs, const dgbgk_par
   return DGBGK_OK;
 }
 
-#define HCHECK(h)                            \
-  do {                                       \
-    if (!(h) || !(h)->impl) {                \
-      set_error("NULL handle");              \
-      return DGBGK_EINVAL;                   \
-    }                                        \
+#define HCHECK(h)               \
+  do {                          \
+    if (!(h) || !(h)->impl) {   \
+      set_error("NULL handle"); \
+      return DGBGK_EINVAL;      \
+    }                           \
   } while (0)
 
 int dgbgk_set_state(dgbgk_handle* h, const double* disnf) {

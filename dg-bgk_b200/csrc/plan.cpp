@@ -146,13 +146,13 @@ int build_plan(const dgbgk_mesh& m, const dgbgk_vspace& vs, const dgbgk_params& 
         inflow_pt[q] = 1;
       }
     }
-  pl.geo.assign(E, ElemGeo<double>{});
+  pl.geo.assign(E, PlanGeo());
   pl.cmax.assign(3 * (size_t)E, 0);
   pl.cmin.assign(3 * (size_t)E, 0);
   for (int en = 0; en < E; ++en) {
     int eo = pl.perm[en];
     const double* G = &m.geome[7 * (size_t)eo];
-    ElemGeo<double>& g = pl.geo[en];
+    PlanGeo& g = pl.geo[en];
     for (int k = 0; k < 3; ++k) {
       g.gx[k] = G[k];
       g.gy[k] = G[k + 3];
@@ -174,7 +174,7 @@ int build_plan(const dgbgk_mesh& m, const dgbgk_vspace& vs, const dgbgk_params& 
   }
 
   // ---- element edges from the side table
-  pl.edge.assign(3 * (size_t)E, ElemEdge<double>{0, 0, 0, -1, -1});
+  pl.edge.assign(3 * (size_t)E, PlanEdge{});
   std::vector<char> seen(3 * (size_t)E, 0);
   // GETBOU's boundary-side lookup: the first BSIDO entry with the side's
   // element and first node (src/getbou.f90:48-53)
@@ -191,7 +191,7 @@ int build_plan(const dgbgk_mesh& m, const dgbgk_vspace& vs, const dgbgk_params& 
     size_t il = 3 * (size_t)enl + kl;
     if (seen[il]) return fail(DGBGK_EMESH, "dgbgk_create: element edge claimed by two sides");
     seen[il] = 1;
-    ElemEdge<double>& L = pl.edge[il];
+    PlanEdge& L = pl.edge[il];
     if (ier > 0) {
       if (I[6] < 1 || I[6] > 3 || I[7] < 1 || I[7] > 3)
         return fail(DGBGK_EMESH, "dgbgk_create: ISIDE right local nodes out of range");
@@ -200,20 +200,20 @@ int build_plan(const dgbgk_mesh& m, const dgbgk_vspace& vs, const dgbgk_params& 
       size_t ir = 3 * (size_t)enr + kr;
       if (seen[ir]) return fail(DGBGK_EMESH, "dgbgk_create: element edge claimed by two sides");
       seen[ir] = 1;
-      ElemEdge<double>& Rr = pl.edge[ir];
+      PlanEdge& Rr = pl.edge[ir];
       double alen = sixth * m.el[s];
       L.nx = m.nx[s];
       L.ny = m.ny[s];
       L.alen = alen;
       L.nbr = enr;
       // my point k = IP1 <-> right's INR1; my point k+1 = IP2 <-> INR2
-      L.info = 0 | 4 | ((I[6] - 1) << 3) | ((I[7] - 1) << 5);
+      L.low = 0 | 4 | ((I[6] - 1) << 3) | ((I[7] - 1) << 5);
       Rr.nx = -m.nx[s];
       Rr.ny = -m.ny[s];
       Rr.alen = alen;
       Rr.nbr = enl;
       // my point k = IP2 <-> left's INL2; my point k+1 = IP1 <-> INL1
-      Rr.info = 0 | ((I[5] - 1) << 3) | ((I[4] - 1) << 5);
+      Rr.low = 0 | ((I[5] - 1) << 3) | ((I[4] - 1) << 5);
     } else {
       auto it = bfind.find({iel, ip1});
       if (it == bfind.end())
@@ -225,7 +225,8 @@ int build_plan(const dgbgk_mesh& m, const dgbgk_vspace& vs, const dgbgk_params& 
       L.ny = m.rsido[3 * b + 1];
       L.alen = sixth * m.rsido[3 * b + 2];
       L.nbr = -1;
-      L.info = kind | (b << 8);
+      L.low = kind;
+      L.bside = b;
       if (kind == 3) pl.has_wall_incoming = true;
     }
   }

@@ -9,6 +9,23 @@
 
 namespace dgbgk {
 
+// Element edge before blocking: the device record ElemEdge<T> packs `low`
+// with the neighbour's tile slot (interior) or `bside` (boundary) into info.
+struct PlanEdge {
+  double nx = 0, ny = 0, alen = 0;
+  int low = -1;   // info bits [0,7): kind, left flag, neighbour local nodes
+  int nbr = -1;   // neighbour element (plan order) or -1
+  int bside = -1; // boundary side index or -1
+};
+
+// Velocity-independent data of one element (FP64 master copy).
+struct PlanGeo {
+  double gx[3] = {0, 0, 0}, gy[3] = {0, 0, 0};  // GEOME(1:3), GEOME(4:6)
+  double area = 0;                              // 0.5 * GEOME(7)
+  double mm[3] = {0, 0, 0};  // MMAT (IMMAT = 1) or CMMAT row sums (IMMAT = 0)
+  int inflow = 0;            // bit i: DG node i sits on an inflow-side node
+};
+
 struct Plan {
   int E = 0, NP = 0, B = 0, S = 0, V = 0, RORDER = 0, TORDER = 0;
   int immat = 1;
@@ -19,10 +36,10 @@ struct Plan {
   // sweep blocking
   int EB = 0, nblocks = 0, max_halo = 0;
   std::vector<int> halo_off, halo_list;  // per block, plan order
-  std::vector<int> eslot;                // [3E] smem slot of the neighbour
+  std::vector<int> eslot;                // [3E] tile slot of the neighbour
   // per element (plan order), FP64 master copies
-  std::vector<ElemGeo<double>> geo;
-  std::vector<ElemEdge<double>> edge;       // [3E]
+  std::vector<PlanGeo> geo;
+  std::vector<PlanEdge> edge;               // [3E]
   std::vector<double> cmax, cmin;           // [3E], IMMAT = 0 residual
   // per velocity
   std::vector<double> cx, cy, wjf, nfinf;
@@ -34,6 +51,13 @@ struct Plan {
   std::vector<int> node_off, node_dg;  // DG node index (plan order) per entry
   std::vector<double> node_ae;         // GEOME(7) of its element
 };
+
+// Device edge word: low bits | (slot or boundary side) << 8.
+inline int edge_info(const Plan& pl, size_t i) {
+  const PlanEdge& e = pl.edge[i];
+  const int hi = ((e.low & 3) == 0) ? pl.eslot[i] : e.bside;
+  return e.low | (hi << 8);
+}
 
 // Builds the plan; returns 0 or a DGBGK_E* code with the message in *err.
 int build_plan(const dgbgk_mesh& m, const dgbgk_vspace& vs, const dgbgk_params& p, int EB, Plan& out,

@@ -9,10 +9,13 @@ import numpy as np
 from conftest import GOLDEN
 
 
-def rel_l2(a, b):
+def rel_l2(a, b, scale=0.0):
+    """||a - b|| / max(||b||, scale * sqrt(n)).  `scale` floors the
+    denominator for fields that can be ~0 (a bulk velocity at rest is
+    compared on the thermal-speed scale, not relative to its own size)."""
     a = np.asarray(a, dtype=np.float64).ravel()
     b = np.asarray(b, dtype=np.float64).ravel()
-    den = np.linalg.norm(b)
+    den = max(np.linalg.norm(b), scale * np.sqrt(b.size))
     return float(np.linalg.norm(a - b) / (den if den > 0 else 1.0))
 
 

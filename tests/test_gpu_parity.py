@@ -49,10 +49,18 @@ def pair(case, prec=64, oracle_prec=64, tile_elems=0, lobatto=None):
     return s, o, f0
 
 
+def vscale(s):
+    """Thermal-speed scale sqrt(R T) of the case, the floor for velocity
+    errors (the bulk velocity is ~0 in a gas at rest)."""
+    c = s.case
+    return float(np.sqrt(c.rgas * c.init["T1"]))
+
+
 def compare_macros(s, o, tol):
     a, b = s.macros(), o.macros()
     for k in ("rho", "u", "v", "temp", "ps", "nd"):
-        assert rel_l2(a[k], b[k]) <= tol, (k, rel_l2(a[k], b[k]))
+        sc = vscale(s) if k in ("u", "v") else 0.0
+        assert rel_l2(a[k], b[k], sc) <= tol, (k, rel_l2(a[k], b[k], sc))
 
 
 def small_cavity():
@@ -83,8 +91,8 @@ def test_moments_and_wall_flux(mk):
     ref = o.compmu()
     got = s.node_fields()
     assert rel_l2(got["disnd"].ravel(), ref["DISND"]) <= 1e-13
-    assert rel_l2(got["disux"].ravel(), ref["DISUX"]) <= 1e-12
-    assert rel_l2(got["disuy"].ravel(), ref["DISUY"]) <= 1e-12
+    assert rel_l2(got["disux"].ravel(), ref["DISUX"], vscale(s)) <= 1e-13
+    assert rel_l2(got["disuy"].ravel(), ref["DISUY"], vscale(s)) <= 1e-13
     assert rel_l2(got["disps"].ravel(), ref["DISPS"]) <= 1e-13
     assert rel_l2(got["mu"].ravel(), ref["MU"]) <= 1e-13
     eta = s.wall_eta()
@@ -105,7 +113,7 @@ def test_fp64_steps_match_oracle(mk, steps):
     compare_macros(s, o, TOL64)
 
 
-@pytest.mark.parametrize("tile", [8, 16, 32, 64])
+@pytest.mark.parametrize("tile", [16, 24, 32, 48, 64])
 def test_tile_shapes_agree(tile):
     s, o, f0 = pair(small_channel(), tile_elems=tile)
     s.advance(3)
@@ -134,7 +142,7 @@ def test_fp32_path_against_fp64_oracle():
     assert rel_l2(s.get_state(), o.get_state()) <= 1e-5
     a, b = s.macros(), o.macros()
     for k in ("rho", "u", "v", "temp"):
-        assert rel_l2(a[k], b[k]) <= 1e-5, k
+        assert rel_l2(a[k], b[k], vscale(s) if k in ("u", "v") else 0.0) <= 1e-5, k
 
 
 def test_early_stop_on_tolerance():

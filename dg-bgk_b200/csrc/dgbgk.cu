@@ -10,6 +10,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -81,6 +82,8 @@ struct ImplBase {
   virtual int wall_eta(double* eta) = 0;
   virtual void info(int* out) = 0;
   virtual int profile(int nsteps, double* ms) = 0;
+  virtual int macros_noalloc(double* scratch, double* nd, double* rho, double* u, double* v, double* ps,
+                             double* temp) = 0;
   Plan pl;
   int device = 0;
   int prec = 64;
@@ -736,6 +739,28 @@ template <class T> struct Impl : ImplBase {
     return 0;
   }
 
+  // dgbgk_get_macros without any allocation: the nodal fields are staged in
+  // the caller-supplied device scratch (the library's static array) and
+  // copied straight into the caller's host arrays.
+  int macros_noalloc(double* scratch, double* nd, double* rho, double* u, double* v, double* ps,
+                     double* temp) override {
+    CK(cudaSetDevice(device));
+    TRY(moments_now());
+    const int NP = pl.NP;
+    NodalArgs a{node_off, node_dg, node_ae, nraw,          disux,  disuy,          disps,
+                scratch,  scratch + NP, scratch + 2 * NP, scratch + 3 * NP, scratch + 4 * NP,
+                scratch + 5 * NP, NP, pl.M / 6.022e26, pl.rgas};
+    k_nodal<<<(NP + 255) / 256, 256, 0, st>>>(a);
+    CK(cudaGetLastError());
+    double* dsts[6] = {nd, rho, u, v, ps, temp};
+    for (int k = 0; k < 6; ++k)
+      if (dsts[k])
+        CK(cudaMemcpyAsync(dsts[k], scratch + (size_t)k * NP, NP * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&hctrl[1], ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return finish_status(hctrl[1]);
+  }
+
   int node_fields(double* nd, double* ux, double* uy, double* ps, double* muo) override {
     CK(cudaSetDevice(device));
     TRY(moments_now());
@@ -938,5 +963,56 @@ int dgbgk_profile_steps(dgbgk_handle* h, int nsteps, double* kernel_ms) {
   return h->impl->profile(nsteps, kernel_ms);
 }
 void dgbgk_destroy(dgbgk_handle* h) { delete h; }
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// dgbgk_get_macros_noalloc: scratch in a file-scope device array.
+//
+// The array lives in every GPU's memory that loads this library, for the
+// life of the process (6 * DGBGK_NOALLOC_MAX_NPOIN doubles, ~6.3 MB).  Host
+// code must not use its name as a pointer (that is a host-side stand-in);
+// the device address is taken once per device with cudaGetSymbolAddress
+// while that device is current, on the first call made on the device.
+// The nodal gather writes every one of the 6*NPOIN entries it uses, so no
+// part of the array needs clearing between calls.
+static __device__ __align__(256) double g_macros_scratch[6 * DGBGK_NOALLOC_MAX_NPOIN];
+
+namespace {
+constexpr int kMaxDevices = 64;
+double* g_macros_scratch_dev[kMaxDevices] = {};
+std::mutex g_macros_scratch_mu;
+
+int macros_scratch_on(int device, double** out) {
+  if (device < 0 || device >= kMaxDevices) {
+    set_error("dgbgk_get_macros_noalloc: device ordinal out of range");
+    return DGBGK_EINVAL;
+  }
+  std::lock_guard<std::mutex> lock(g_macros_scratch_mu);
+  if (!g_macros_scratch_dev[device]) {
+    void* p = nullptr;
+    CK(cudaSetDevice(device));
+    CK(cudaGetSymbolAddress(&p, g_macros_scratch));
+    g_macros_scratch_dev[device] = static_cast<double*>(p);
+  }
+  *out = g_macros_scratch_dev[device];
+  return 0;
+}
+}  // namespace
+
+extern "C" {
+
+int dgbgk_get_macros_noalloc(dgbgk_handle* h, double* nd, double* rho, double* u, double* v, double* ps,
+                             double* temp) {
+  HCHECK(h);
+  if (h->impl->pl.NP > DGBGK_NOALLOC_MAX_NPOIN) {
+    set_error("dgbgk_get_macros_noalloc: NPOIN = " + std::to_string(h->impl->pl.NP) +
+              " exceeds DGBGK_NOALLOC_MAX_NPOIN = " + std::to_string(DGBGK_NOALLOC_MAX_NPOIN));
+    return DGBGK_EINVAL;
+  }
+  double* scratch = nullptr;
+  TRY(macros_scratch_on(h->impl->device, &scratch));
+  return h->impl->macros_noalloc(scratch, nd, rho, u, v, ps, temp);
+}
 
 }  // extern "C"

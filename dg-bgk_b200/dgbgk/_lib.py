@@ -70,6 +70,7 @@ SIGNATURES = {
     "dgbgk_set_residual_reference": (c_int, [c_void_p, c_double]),
     "dgbgk_get_residual_reference": (c_int, [c_void_p, _PD]),
     "dgbgk_get_macros": (c_int, [c_void_p, _PD, _PD, _PD, _PD, _PD, _PD]),
+    "dgbgk_get_macros_noalloc": (c_int, [c_void_p, _PD, _PD, _PD, _PD, _PD, _PD]),
     "dgbgk_get_node_fields": (c_int, [c_void_p, _PD, _PD, _PD, _PD, _PD]),
     "dgbgk_get_wall_eta": (c_int, [c_void_p, _PD]),
     "dgbgk_info": (c_int, [c_void_p, _PI]),

@@ -173,6 +173,23 @@ int dgbgk_last_timing(dgbgk_handle* h, double* total_ms);
  * state advances by nsteps steps exactly as under dgbgk_advance(). */
 int dgbgk_profile_steps(dgbgk_handle* h, int nsteps, double* kernel_ms);
 
+/* No counterpart in the reference.  dgbgk_get_macros() without any device
+ * allocation, for callers that cannot allocate GPU memory at call time: a
+ * host whose device memory is owned by another allocator or pool, a time
+ * loop that must not pay the device-wide synchronisation of cudaMalloc /
+ * cudaFree while other streams run, or code that runs after its memory
+ * budget is fixed.  The nodal fields are staged in one static device array
+ * of 6*DGBGK_NOALLOC_MAX_NPOIN doubles (~6.3 MB) that every GPU loading the
+ * library holds until the process exits; meshes with NPOIN above the limit
+ * are rejected with DGBGK_EINVAL.  The first call on a device takes the
+ * array's device address (cudaGetSymbolAddress) and should come before any
+ * stream capture.  All calls share the one array: calls that overlap on the
+ * GPU (from several handles or threads on the same device) race and must
+ * be serialised by the caller. */
+#define DGBGK_NOALLOC_MAX_NPOIN 131072
+int dgbgk_get_macros_noalloc(dgbgk_handle* h, double* nd, double* rho, double* u, double* v, double* ps,
+                             double* temp);
+
 void dgbgk_destroy(dgbgk_handle* h);
 const char* dgbgk_last_error(void);
 

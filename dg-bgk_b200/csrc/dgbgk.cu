@@ -1,9 +1,6 @@
 // C ABI of the DG-BGK sweep on B200 (sm_100a): handle management, device
-// memory, TMA descriptors, the captured two-step CUDA graph and the state
-// transfers.
-#include <cuda.h>
+// memory, the captured two-step CUDA graph and the state transfers.
 #include <cuda_runtime.h>
-#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <cmath>
@@ -58,18 +55,6 @@ template <class X> void dfree(X*& p) {
   p = nullptr;
 }
 
-PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
-  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-  if (!fn) {
-    cudaDriverEntryPointQueryResult q;
-    void* p = nullptr;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
-  }
-  return fn;
-}
-
 struct ImplBase {
   virtual ~ImplBase() {}
   virtual int set_state(const void* src, bool f32) = 0;
@@ -93,16 +78,14 @@ struct ImplBase {
 };
 
 template <class T> struct Impl : ImplBase {
-  static constexpr int TY = 8;  // warps per sweep CTA
   cudaStream_t st = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, evpoll[2] = {nullptr, nullptr};
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
   int cur = 0;
-  int M = 4;
+  int tpu = 1;  // velocity tiles per sweep work unit
   int Vp = 0;
   // device arrays
   T* f[2] = {nullptr, nullptr};
-  CUtensorMap tm_blk[2], tm_row3[2];
   ElemRec<T>* rec = nullptr;
   int *halo_off = nullptr, *halo_list = nullptr;
   T *cmax = nullptr, *cmin = nullptr;
@@ -174,10 +157,9 @@ template <class T> struct Impl : ImplBase {
     if (st) cudaStreamDestroy(st);
   }
 
-  int nvt() const { return (pl.V + VTILE - 1) / VTILE; }
-  static int default_m() { return sizeof(T) == 8 ? 3 : 6; }
-  int slots() const { return pl.EB + pl.max_halo; }
-  size_t sweep_smem() const { return SweepSmem<T>(pl.EB, slots()).total; }
+  int nvt() const { return (pl.V + SweepGeo<T>::VT - 1) / SweepGeo<T>::VT; }
+  static int default_eb() { return 128; }
+  size_t sweep_smem() const { return SweepGeo<T>::smem(pl.EB, pl.max_halo); }
 
   int init(int tile_elems) {
     CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
@@ -200,8 +182,13 @@ template <class T> struct Impl : ImplBase {
     TRY(dalloc(&disuy, ndg));
     TRY(dalloc(&disps, ndg));
     TRY(dalloc(&mu, ndg));
-    std::vector<T> a(pl.cx.begin(), pl.cx.end()), b(pl.cy.begin(), pl.cy.end()),
-        c(pl.nfinf.begin(), pl.nfinf.end());
+    // sweep velocity tables, zero past V
+    std::vector<T> a(Vp, (T)0), b(Vp, (T)0), c(Vp, (T)0);
+    for (int v = 0; v < pl.V; ++v) {
+      a[v] = (T)pl.cx[v];
+      b[v] = (T)pl.cy[v];
+      c[v] = (T)pl.nfinf[v];
+    }
     TRY(upload(&cxT, a, st));
     TRY(upload(&cyT, b, st));
     TRY(upload(&nfT, c, st));
@@ -272,49 +259,22 @@ template <class T> struct Impl : ImplBase {
     return 0;
   }
 
-  template <int MM> int sweep_occupancy(int* per_sm) {
-    CK(cudaFuncSetAttribute(k_sweep<T, MM, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sweep_smem()));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_sweep<T, MM, TY>, 32 * TY, sweep_smem()));
-    return 0;
+  using SweepFn = void (*)(SweepArgs<T>);
+  SweepFn sweep_fn() const {
+    if (pl.EB == 64) return pl.immat == 1 ? k_sweep<T, 64, 1> : k_sweep<T, 64, 0>;
+    return pl.immat == 1 ? k_sweep<T, 128, 1> : k_sweep<T, 128, 0>;
   }
 
-  int make_tensor_maps() {
-    auto enc = tensor_map_encoder();
-    if (!enc) {
-      set_error("cuTensorMapEncodeTiled is not available from the driver");
-      return DGBGK_ECUDA;
-    }
-    const CUtensorMapDataType dt = sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
-    cuuint64_t dims[2] = {(cuuint64_t)pl.V, (cuuint64_t)3 * pl.E};
-    cuuint64_t strides[1] = {(cuuint64_t)Vp * sizeof(T)};
-    cuuint32_t estr[2] = {1, 1};
-    for (int b = 0; b < 2; ++b) {
-      cuuint32_t box_blk[2] = {(cuuint32_t)VTILE, (cuuint32_t)(3 * pl.EB)};
-      cuuint32_t box_row[2] = {(cuuint32_t)VTILE, 3u};
-      CUresult r1 = enc(&tm_blk[b], dt, 2, f[b], dims, strides, box_blk, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                        CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-      CUresult r2 = enc(&tm_row3[b], dt, 2, f[b], dims, strides, box_row, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                        CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-      if (r1 != CUDA_SUCCESS || r2 != CUDA_SUCCESS) {
-        set_error("cuTensorMapEncodeTiled failed for the state buffer");
-        return DGBGK_ECUDA;
-      }
-    }
-    return 0;
-  }
-
-  // Sweep tile: elements per CTA = 8 warps x M elements per warp.
+  // Sweep tile: EB elements per CTA (2*EB threads) x one 64-byte velocity
+  // segment.
   int set_tile(int tile_elems) {
-    const int m = tile_elems > 0 ? tile_elems / TY : default_m();
-    if ((m != 2 && m != 3 && m != 4 && m != 6 && m != 8) || (tile_elems > 0 && tile_elems % TY)) {
-      set_error("tile_elems must be 16, 24, 32, 48 or 64");
+    const int eb = tile_elems > 0 ? tile_elems : default_eb();
+    if (eb != 64 && eb != 128) {
+      set_error("tile_elems must be 64 or 128");
       return DGBGK_EINVAL;
     }
-    M = m;
-    if (pl.EB != TY * M || halo_off == nullptr) {
-      build_blocks(pl, TY * M);
+    if (pl.EB != eb || halo_off == nullptr) {
+      build_blocks(pl, eb);
       dfree(halo_off);
       dfree(halo_list);
       dfree(rec);
@@ -326,6 +286,7 @@ template <class T> struct Impl : ImplBase {
       std::memset((void*)r.data(), 0, r.size() * sizeof(ElemRec<T>));
       for (int e = 0; e < pl.E; ++e) {
         const auto& g = pl.geo[e];
+        int flags = g.inflow & 7;
         for (int k = 0; k < 3; ++k) {
           r[e].gx[k] = (T)g.gx[k];
           r[e].gy[k] = (T)g.gy[k];
@@ -334,10 +295,13 @@ template <class T> struct Impl : ImplBase {
           r[e].edge[k].nx = (T)pl.edge[i].nx;
           r[e].edge[k].ny = (T)pl.edge[i].ny;
           r[e].edge[k].alen = (T)pl.edge[i].alen;
-          r[e].edge[k].info = edge_info(pl, i);
+          r[e].edge[k].info = edge_info(pl, i, e % eb);
+          const bool wall = (pl.edge[i].low & 3) == 3;
+          r[e].bside[k] = wall ? pl.edge[i].bside : -1;
+          if (wall) flags |= 8 << k;
         }
         r[e].area = (T)g.area;
-        r[e].inflow = g.inflow;
+        r[e].flags = flags;
       }
       TRY(upload(&rec, r, st));
     }
@@ -345,21 +309,23 @@ template <class T> struct Impl : ImplBase {
       set_error("sweep tile needs more than 227 KB of shared memory");
       return DGBGK_EUNSUP;
     }
-    TRY(make_tensor_maps());
+    SweepFn fn = sweep_fn();
+    CK(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sweep_smem()));
     int per_sm = 0;
-    switch (M) {
-      case 2: TRY(sweep_occupancy<2>(&per_sm)); break;
-      case 3: TRY(sweep_occupancy<3>(&per_sm)); break;
-      case 4: TRY(sweep_occupancy<4>(&per_sm)); break;
-      case 6: TRY(sweep_occupancy<6>(&per_sm)); break;
-      default: TRY(sweep_occupancy<8>(&per_sm)); break;
-    }
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)fn, 2 * pl.EB, sweep_smem()));
     if (per_sm < 1) {
       set_error("sweep kernel does not fit on an SM with this tile");
       return DGBGK_EUNSUP;
     }
-    const int ntiles = pl.nblocks * nvt();
-    sweep_grid = std::max(1, std::min(ntiles, per_sm * nsm));
+    // velocity tiles per work unit: about eight units per resident CTA, so
+    // the dynamic hand-out balances, and equal groups of tiles
+    const int grid0 = per_sm * nsm;
+    const long total = (long)pl.nblocks * nvt();
+    tpu = (int)std::min<long>(SweepGeo<T>::TPU_MAX, std::max<long>(1, total / (8L * grid0)));
+    const int ngroups = (nvt() + tpu - 1) / tpu;
+    tpu = (nvt() + ngroups - 1) / ngroups;
+    const int nunits = pl.nblocks * ngroups;
+    sweep_grid = std::max(1, std::min(nunits, grid0));
     if (sweep_grid > part_cap) {
       dfree(part_max);
       dfree(part_sq);
@@ -418,6 +384,7 @@ template <class T> struct Impl : ImplBase {
   }
   int launch_sweep(int src) {
     SweepArgs<T> a;
+    a.fin = f[src];
     a.fout = f[1 - src];
     a.rec = rec;
     a.halo_off = halo_off;
@@ -436,22 +403,13 @@ template <class T> struct Impl : ImplBase {
     a.E = pl.E;
     a.V = pl.V;
     a.Vp = Vp;
-    a.EB = pl.EB;
-    a.slots = slots();
     a.nblocks = pl.nblocks;
+    a.max_halo = pl.max_halo;
     a.nvt = nvt();
-    a.immat = pl.immat;
+    a.tpu = tpu;
     a.alpha = (T)pl.alpha;
     a.rgas = (T)pl.rgas;
-    const dim3 block(32, TY);
-    const size_t smem = sweep_smem();
-    switch (M) {
-      case 2: k_sweep<T, 2, TY><<<sweep_grid, block, smem, st>>>(tm_blk[src], tm_row3[src], a); break;
-      case 3: k_sweep<T, 3, TY><<<sweep_grid, block, smem, st>>>(tm_blk[src], tm_row3[src], a); break;
-      case 4: k_sweep<T, 4, TY><<<sweep_grid, block, smem, st>>>(tm_blk[src], tm_row3[src], a); break;
-      case 6: k_sweep<T, 6, TY><<<sweep_grid, block, smem, st>>>(tm_blk[src], tm_row3[src], a); break;
-      default: k_sweep<T, 8, TY><<<sweep_grid, block, smem, st>>>(tm_blk[src], tm_row3[src], a); break;
-    }
+    sweep_fn()<<<sweep_grid, 2 * pl.EB, sweep_smem(), st>>>(a);
     CK(cudaGetLastError());
     return 0;
   }
@@ -805,7 +763,7 @@ template <class T> struct Impl : ImplBase {
     o[4] = pl.V;
     o[5] = prec;
     o[6] = pl.EB;
-    o[7] = VTILE;
+    o[7] = SweepGeo<T>::VT;
     o[8] = pl.nblocks;
     o[9] = pl.max_halo;
   }
@@ -858,7 +816,7 @@ int dgbgk_create(const dgbgk_mesh* mesh, const dgbgk_vspace* vs, const dgbgk_par
   impl->device = prm->device;
   impl->prec = prm->precision;
   std::string err;
-  const int eb0 = prm->tile_elems > 0 ? prm->tile_elems : (prm->precision == 64 ? 24 : 48);
+  const int eb0 = prm->tile_elems > 0 ? prm->tile_elems : 128;
   int rc = build_plan(*mesh, *vs, *prm, eb0, impl->pl, &err);
   if (rc != 0) {
     set_error(err);

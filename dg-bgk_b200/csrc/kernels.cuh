@@ -11,20 +11,21 @@
 //   k_wall    : FLUCON2 (src/flucon2.f90:134-233), one warp per wall side.
 //   k_sweep   : the whole velocity-loop body (GTEQNF, GETFLA, GETELC,
 //               EDGFLXOPT/GETBOU, GETINC/CMMINC, ADTHEM, INFLOW;
-//               src/advnce.f90:286-377) on tiles of (element block x 32
-//               velocities).  Persistent CTAs; each tile's inputs -- the
-//               block's f rows in one 2-D TMA box, each halo element's rows
-//               in a 3-row box, the block's element records in one bulk copy
-//               and the halo's record heads -- land in a two-stage
-//               shared-memory ring while the previous tile is computed.
+//               src/advnce.f90:286-377) on tiles of (element block x one
+//               64-byte velocity segment).  Persistent CTAs draw work units
+//               (a block at several tiles); the block's records are staged
+//               once per unit, the tiles' f rows (block and halo) arrive by
+//               double-buffered cp.async copies, and each thread works on
+//               whole elements at 8 (FP32) or 4 (FP64) velocities.
 //   k_resid   : GETRES + the residual bookkeeping (src/advnce.f90:385,
 //               422-429), the convergence test and the step counter.
-// Every device-side wait is bounded: on expiry the kernel sets
-// Ctrl::timeout, drains its own copies with a second bounded wait and
+// Every device-side wait on an mbarrier is bounded: on expiry the kernel
+// sets Ctrl::timeout, drains its own copies with a second bounded wait and
 // returns; the host reports DGBGK_ECUDA.
 #pragma once
-#include <cuda.h>
 #include <cuda_runtime.h>
+
+#include <type_traits>
 
 #include "types.h"
 
@@ -32,6 +33,7 @@ namespace dgbgk {
 
 constexpr double PI_D = 3.1416;  // the reference's PI
 constexpr double TINY_D = 1e-20;
+constexpr double LOG2E_D = 1.4426950408889634;  // log2(e)
 constexpr unsigned WAIT_TRIES = 1u << 22;  // x ~256 ns sleep: ~1 s
 
 // e^x in FP32 for the FP32 sweep: t = x*log2(e) is formed with its rounding
@@ -97,14 +99,6 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
     if (i > 32) __nanosleep(256);
   }
   return false;
-}
-// 2-D tiled TMA load (no multicast) of box {x, y} into shared memory.
-__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
-          smem_u32(dst)),
-      "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar))
-      : "memory");
 }
 // 1-D bulk copy global -> shared (16-byte aligned, size a multiple of 16).
 __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
@@ -290,10 +284,10 @@ __global__ void __launch_bounds__(512) k_moments(MomArgs<T> a) {
         const double rho = a.MM * nd;
         const double b2 = rho / (2 * ps);
         en.A[i] = (T)(nd * (b2 / PI_D));
-        en.B[i] = (T)b2;
+        en.ex[i] = (T)(sizeof(T) == 4 ? -b2 * LOG2E_D : -b2);
       } else {
         en.A[i] = (T)0;
-        en.B[i] = (T)0;
+        en.ex[i] = (T)0;
       }
       en.ux[i] = (T)ux;
       en.uy[i] = (T)uy;
@@ -348,13 +342,14 @@ template <class T> __global__ void __launch_bounds__(256) k_wall(WallArgs<T> a) 
 
 // -------------------------------------------------------------- sweep ----
 template <class T> struct SweepArgs {
+  const T* __restrict__ fin;
   T* __restrict__ fout;
   const ElemRec<T>* __restrict__ rec;
   const int* __restrict__ halo_off;
   const int* __restrict__ halo_list;
-  const T* __restrict__ cx;
-  const T* __restrict__ cy;
-  const T* __restrict__ nfinf;
+  const T* __restrict__ cx;     // [Vp], zero past V
+  const T* __restrict__ cy;     // [Vp], zero past V
+  const T* __restrict__ nfinf;  // [Vp], zero past V
   const T* __restrict__ bTw;
   const T* __restrict__ bUw;
   const T* __restrict__ bEta;
@@ -363,7 +358,9 @@ template <class T> struct SweepArgs {
   double* __restrict__ part_max;
   double* __restrict__ part_sq;
   Ctrl* ctrl;
-  int E, V, Vp, EB, slots, nblocks, nvt, immat;
+  int E, V, Vp, nblocks, max_halo;
+  int nvt;  // velocity tiles holding some v < V
+  int tpu;  // velocity tiles per work unit (<= SweepGeo::TPU_MAX)
   T alpha, rgas;
 };
 
@@ -374,268 +371,433 @@ __device__ __forceinline__ double step_dt(const Ctrl* c) {
   return fmin(dtb, c->dtc);
 }
 
-// NFO of DG node i (src/gteqnf.f90:324-326)
-template <class T>
-__device__ __forceinline__ T feq_of(const ElemRec<T>& r, int i, T cx, T cy) {
-  const T dx = r.ux[i] - cx, dy = r.uy[i] - cy;
-  return r.A[i] * dexp<T>(-r.B[i] * (dx * dx + dy * dy));
-}
-
-// UMEAN of one element at one velocity (src/getelc.f90:54-83):
-// 0.5*DTE*(div F - 1/3 sum MU (NFO - f)), div F = sum (N_i,x cx + N_i,y cy) f_i.
-template <class T>
-__device__ __forceinline__ T umean_of(const T* f, const T* q, const ElemRec<T>& r, T cx, T cy, T dth) {
-  const T dive = (r.gx[0] * cx + r.gy[0] * cy) * f[0] + (r.gx[1] * cx + r.gy[1] * cy) * f[1] +
-                 (r.gx[2] * cx + r.gy[2] * cy) * f[2];
-  const T coll = r.mu[0] * (q[0] - f[0]) + r.mu[1] * (q[1] - f[1]) + r.mu[2] * (q[2] - f[2]);
-  return (dive - coll * (T)(1.0 / 3.0)) * dth;
-}
-
-// Shared-memory carve-up of one sweep CTA (bytes): two stages, each =
-// f rows [slots][3][32] + element records [EB] + halo record heads
-// [slots-EB], 128-aligned; then the UMEAN tile [slots][32]; + 128 bytes of
-// slack to align the base at run time.
-template <class T> struct SweepSmem {
-  unsigned f_bytes, rec_bytes, halo_bytes, stage_bytes, um_bytes, total;
-  __host__ __device__ SweepSmem(int EB, int slots) {
-    f_bytes = (unsigned)(slots * 3 * VTILE * sizeof(T));
-    rec_bytes = (unsigned)(EB * sizeof(ElemRec<T>));
-    halo_bytes = (unsigned)((slots - EB) * umean_part_bytes<T>());
-    stage_bytes = (f_bytes + rec_bytes + halo_bytes + 127) / 128 * 128;
-    um_bytes = (unsigned)(slots * VTILE * sizeof(T));
-    total = 2 * stage_bytes + um_bytes + 128;
+// Sweep tile geometry.  A tile is one 64-byte segment of velocities (16 FP32
+// or 8 FP64 values) of the three rows of every element of a block and of its
+// halo.  In shared memory an element's three 64-byte row segments sit at an
+// element pitch of 208 bytes, an odd number of 16-byte units, so eight
+// threads that each read their own element's rows with 16-byte vectors fall
+// on eight distinct bank groups.  A work unit is one block at `tpu`
+// consecutive velocity tiles: the block's element records and the halo's
+// record heads are staged in shared memory once per unit, the f rows once
+// per tile (double-buffered).
+template <class T> struct SweepGeo {
+  static constexpr int W = 16 / (int)sizeof(T);  // values per 16-byte vector
+  static constexpr int VT = 64 / (int)sizeof(T);  // velocities per tile
+  static constexpr int NCH = 4;                   // 16-byte chunks per row segment
+  static constexpr int ER = 208;                  // element pitch of a tile (bytes)
+  static constexpr int RW = (int)(sizeof(ElemRec<T>) / 16);                    // record words
+  static constexpr int HW = (REC_HEAD_VALUES * (int)sizeof(T) + 15) / 16;        // head words
+  static constexpr int HR = 16 * (HW | 1);  // halo head pitch (odd number of words)
+  static constexpr int TPU_MAX = 16;
+  // two tiles [EB + max_halo][ER], records [EB], halo heads [max_halo][HR],
+  // velocity tables cx, cy, NFINF [3][TPU_MAX * VT], halo element list
+  static constexpr size_t smem(int EB, int max_halo) {
+    return 2 * (size_t)(EB + max_halo) * ER + (size_t)EB * sizeof(ElemRec<T>) + (size_t)max_halo * HR +
+           3 * (size_t)TPU_MAX * VT * sizeof(T) + ((size_t)max_halo * 4 + 15) / 16 * 16;
   }
 };
 
-template <class T, int M, int TY>
-__global__ void __launch_bounds__(32 * TY) k_sweep(const __grid_constant__ CUtensorMap tm_blk,
-                                                   const __grid_constant__ CUtensorMap tm_row3,
-                                                   SweepArgs<T> a) {
+// 16-byte asynchronous copy global -> shared through L2 only (cp.async.cg).
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// exp of the NFO exponent: FP64 exp(x); FP32 2^x from the SFU (ex2.approx,
+// relative error ~2^-22; the FP32 coefficient carries the log2(e) factor,
+// applied in FP64 by the moment kernel).
+template <class T> __device__ __forceinline__ T nfo_exp(T x);
+template <> __device__ __forceinline__ double nfo_exp<double>(double x) { return exp(x); }
+template <> __device__ __forceinline__ float nfo_exp<float>(float x) {
+  float p;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(p) : "f"(x));
+  return p;
+}
+
+template <class T> struct Vec;
+template <> struct Vec<float> {
+  using type = float4;
+  static __device__ __forceinline__ float get(const float4& v, int k) {
+    return k == 0 ? v.x : k == 1 ? v.y : k == 2 ? v.z : v.w;
+  }
+  static __device__ __forceinline__ void set(float4& v, int k, float x) {
+    if (k == 0)
+      v.x = x;
+    else if (k == 1)
+      v.y = x;
+    else if (k == 2)
+      v.z = x;
+    else
+      v.w = x;
+  }
+};
+template <> struct Vec<double> {
+  using type = double2;
+  static __device__ __forceinline__ double get(const double2& v, int k) { return k == 0 ? v.x : v.y; }
+  static __device__ __forceinline__ void set(double2& v, int k, double x) {
+    if (k == 0)
+      v.x = x;
+    else
+      v.y = x;
+  }
+};
+template <class T> __device__ __forceinline__ typename Vec<T>::type vld(const void* p) {
+  return *reinterpret_cast<const typename Vec<T>::type*>(p);
+}
+template <class T> __device__ __forceinline__ void vst(void* p, const typename Vec<T>::type& v) {
+  *reinterpret_cast<typename Vec<T>::type*>(p) = v;
+}
+
+// Phase 1 of the sweep on one 16-byte chunk of an element's three rows in
+// the tile: NFO (GTEQNF, src/gteqnf.f90:324-326) and UMEAN =
+// 0.5*DTE*(div F - 1/3 sum_i MU_i (NFO_i - f_i)) with div F = sum_i
+// (N_i,x cx + N_i,y cy) f_i (GETELC, src/getelc.f90:54-83).  The rows are
+// overwritten in place with g = f - UMEAN, the value every edge flux and the
+// volume term of this element use (src/getelc.f90:87-117,
+// src/edgflxopt.f90:95-125); NFO and UMEAN are returned.
+template <class T>
+__device__ __forceinline__ void sweep_p1(const ElemRec<T>& r, unsigned char* row, const typename Vec<T>::type& cxv,
+                                         const typename Vec<T>::type& cyv, T dth, T dth3,
+                                         typename Vec<T>::type (&q)[3], typename Vec<T>::type& u) {
+  using VO = Vec<T>;
+  constexpr int W = SweepGeo<T>::W;
+  typename VO::type f[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) f[i] = vld<T>(row + 64 * i);
+#pragma unroll
+  for (int w = 0; w < W; ++w) {
+    const T cx = VO::get(cxv, w), cy = VO::get(cyv, w);
+    const T f0 = VO::get(f[0], w), f1 = VO::get(f[1], w), f2 = VO::get(f[2], w);
+    const T sx = r.gx[0] * f0 + r.gx[1] * f1 + r.gx[2] * f2;
+    const T sy = r.gy[0] * f0 + r.gy[1] * f1 + r.gy[2] * f2;
+    T coll = (T)0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const T dx = r.ux[i] - cx, dy = r.uy[i] - cy;
+      const T qi = r.A[i] * nfo_exp<T>(r.ex[i] * (dx * dx + dy * dy));
+      VO::set(q[i], w, qi);
+      coll += r.mu[i] * (qi - VO::get(f[i], w));
+    }
+    const T um = dth * (sx * cx + sy * cy) - dth3 * coll;
+    VO::set(u, w, um);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) VO::set(f[i], w, VO::get(f[i], w) - um);
+  }
+#pragma unroll
+  for (int i = 0; i < 3; ++i) vst<T>(row + 64 * i, f[i]);
+}
+
+// Persistent sweep kernel: EB block elements, 2*EB threads.  Work units are
+// (block b, group of `tpu` velocity tiles) with b fastest, handed out in
+// order (the first by blockIdx, the rest from a device counter), so the CTAs
+// running at one moment cover neighbouring blocks at the same velocities and
+// the halo rows they read are L2 hits.  Per unit the block's element records
+// and the halo's record heads are staged in shared memory; per tile the
+// three 64-byte row segments of every block and halo element arrive by
+// 16-byte cp.async copies, double-buffered so the next tile's rows load
+// while this one is computed.  Per tile:
+//  * phase 1: UMEAN and g = f - UMEAN of every block and halo element; a
+//    block element's NFO and UMEAN stay in the registers of the thread that
+//    updates it;
+//  * phase 2, thread j and j+EB take half of block element j's velocities
+//    each: the volume term (src/getelc.f90:87-117), the edge fluxes gathered
+//    per element (EDGFLXOPT src/edgflxopt.f90:95-125; outflow and, with zero
+//    length, inflow and wall sides read the element itself), the wall sides'
+//    fluxes (GETBOU src/getbou.f90:142-281), GETINC/CMMINC, ADTHEM and INFLOW;
+//    16-byte vector stores of the new rows.
+// Upwinding: the own value is taken where SC = n.c > 0.  The reference takes
+// it where SC > 0 for the ISIDE(3) element and SC >= 0 for the other; the
+// two differ only at SC = 0, where the flux SC*value is zero either way.
+template <class T, int EB, int IMMAT>
+__global__ void __launch_bounds__(2 * EB, sizeof(T) == 4 ? 2 : 1) k_sweep(SweepArgs<T> a) {
   if (a.ctrl->done) return;
-  constexpr int VT = VTILE;
-  constexpr int EB = TY * M;
-  constexpr unsigned HB = umean_part_bytes<T>();
+  using G = SweepGeo<T>;
+  using VO = Vec<T>;
+  using VecT = typename VO::type;
+  constexpr int W = G::W, VT = G::VT, NCH = G::NCH, ER = G::ER, RW = G::RW, HW = G::HW, HR = G::HR;
+  constexpr int NT = 2 * EB, NW = NT / 32;
+  static_assert(EB % 16 == 0, "whole warps");
   extern __shared__ __align__(128) unsigned char sm_raw[];
-  __shared__ uint64_t bars[2];
-  __shared__ double red_m[TY], red_s[TY];
-  const int tx = threadIdx.x, ty = threadIdx.y;
-  const SweepSmem<T> L(EB, a.slots);
-  // TMA destinations must be 128-byte aligned: align the base at run time
-  unsigned char* base = sm_raw + ((128u - (smem_u32(sm_raw) & 127u)) & 127u);
-  T* um_s = reinterpret_cast<T*>(base + 2 * L.stage_bytes);  // [slots][VT]
-  const int ntiles = a.nblocks * a.nvt;
-  const int G = gridDim.x;
+  __shared__ int s_unit;
+  __shared__ double red_m[NW], red_s[NW];
+  const int tid = threadIdx.x;
+  const int slots = EB + a.max_halo;
+  const size_t tile_bytes = (size_t)slots * ER;
+  ElemRec<T>* const recs = reinterpret_cast<ElemRec<T>*>(sm_raw + 2 * tile_bytes);
+  unsigned char* const hrec = reinterpret_cast<unsigned char*>(recs + EB);
+  T* const vtab = reinterpret_cast<T*>(hrec + (size_t)a.max_halo * HR);  // cx, cy, NFINF
+  constexpr int UV = G::TPU_MAX * VT;
+  int* const hl = reinterpret_cast<int*>(vtab + 3 * UV);  // halo elements of the unit's block
+  const int nvg = (a.nvt + a.tpu - 1) / a.tpu;
+  const int nunits = a.nblocks * nvg;
+  const int j = tid < EB ? tid : tid - EB, hh = tid < EB ? 0 : 1;
 
-  if (tx == 0 && ty == 0) {
-    mbar_init(&bars[0], 1);
-    mbar_init(&bars[1], 1);
-    fence_mbar_init();
-  }
-  __syncthreads();
-
-  // warp 0 issues the copies of tile t into stage s
-  auto issue = [&](int t, int s) {
-    const int b = t % a.nblocks, vt = t / a.nblocks;
-    const int v0 = vt * VT, e0 = b * EB;
-    const int nb = min(EB, a.E - e0);
-    const int h0 = a.halo_off[b], nh = a.halo_off[b + 1] - h0;
-    unsigned char* st = base + s * L.stage_bytes;
-    T* dst = reinterpret_cast<T*>(st);
-    unsigned char* recd = st + L.f_bytes;
-    unsigned char* hald = recd + L.rec_bytes;
-    if (tx == 0) {
-      const unsigned bytes = (unsigned)((3 * EB + 3 * nh) * VT * sizeof(T)) +
-                             (unsigned)(nb * sizeof(ElemRec<T>)) + (unsigned)nh * HB;
-      mbar_expect_tx(&bars[s], bytes);
-      tma_load_2d(dst, &tm_blk, v0, 3 * e0, &bars[s]);
-      bulk_load(recd, a.rec + e0, (unsigned)(nb * sizeof(ElemRec<T>)), &bars[s]);
-    }
-    __syncwarp();
-    for (int h = tx; h < nh; h += 32) {
-      const int e = a.halo_list[h0 + h];
-      tma_load_2d(dst + (size_t)(EB + h) * 3 * VT, &tm_row3, v0, 3 * e, &bars[s]);
-      bulk_load(hald + (size_t)h * HB, a.rec + e, HB, &bars[s]);
-    }
-  };
-
-  int t = blockIdx.x;
-  if (ty == 0) {
-    if (t < ntiles) issue(t, 0);
-    if (t + G < ntiles) issue(t + G, 1);
-  }
   const double dtd = step_dt(a.ctrl);
-  const T dt = (T)dtd, dth = (T)(dtd * 0.5);
+  const T dt = (T)dtd, dth = (T)(0.5 * dtd), dth3 = (T)(0.5 * dtd / 3.0), third = (T)(1.0 / 3.0);
   double rmax = 0.0, rsq = 0.0;
-  uint32_t par = 0;
-  int s = 0;
-  bool aborted = false;
 
-  for (; t < ntiles; t += G) {
-    // every thread waits for the stage itself; a timeout is voted on at the
-    // end-of-tile barrier so that all threads leave together
-    const bool ok = mbar_wait_bounded(&bars[s], (par >> s) & 1);
-    par ^= 1u << s;
-    const unsigned char* st = base + s * L.stage_bytes;
-    const T* fs = reinterpret_cast<const T*>(st);
-    const ElemRec<T>* recs = reinterpret_cast<const ElemRec<T>*>(st + L.f_bytes);
-    const unsigned char* halr = st + L.f_bytes + L.rec_bytes;
-    const int b = t % a.nblocks, vt = t / a.nblocks;
-    const int v = vt * VT + tx;
-    const bool vok = v < a.V;
-    const T cx = vok ? a.cx[v] : (T)0, cy = vok ? a.cy[v] : (T)0;
-    const int e0 = b * EB;
-    const int nb = min(EB, a.E - e0);
-    const int nh = a.halo_off[b + 1] - a.halo_off[b];
+  int unit = blockIdx.x;
+  // the unit after this one, drawn ahead so the atomic's latency is hidden
+  int next = (tid == 0 && unit < nunits) ? (int)gridDim.x + atomicAdd(&a.ctrl->sweep_next, 1) : 0;
+  while (unit < nunits) {
+    const int b = unit % a.nblocks, vg = unit / a.nblocks;
+    const int e0 = b * EB, nb = min(EB, a.E - e0);
+    const int h0 = a.halo_off[b], nh = a.halo_off[b + 1] - h0;
+    const int n = nb + nh;
+    const int vt0 = vg * a.tpu, ntl = min(a.tpu, a.nvt - vt0);
 
-    // phase 1: NFO and N_i,x cx + N_i,y cy of the block (kept in
-    // registers) and UMEAN of block + halo
-    T q[M][3], sv[M][3], um[M];
-#pragma unroll
-    for (int m = 0; m < M; ++m) {
-      const int j = ty + TY * m;
-      if (ok && j < nb) {
-        const ElemRec<T>& r = recs[j];
-        const T f[3] = {fs[(j * 3 + 0) * VT + tx], fs[(j * 3 + 1) * VT + tx], fs[(j * 3 + 2) * VT + tx]};
-#pragma unroll
-        for (int i = 0; i < 3; ++i) {
-          q[m][i] = feq_of(r, i, cx, cy);
-          sv[m][i] = r.gx[i] * cx + r.gy[i] * cy;
-        }
-        const T dive = sv[m][0] * f[0] + sv[m][1] * f[1] + sv[m][2] * f[2];
-        const T coll = r.mu[0] * (q[m][0] - f[0]) + r.mu[1] * (q[m][1] - f[1]) + r.mu[2] * (q[m][2] - f[2]);
-        um[m] = (dive - coll * (T)(1.0 / 3.0)) * dth;
-        um_s[j * VT + tx] = um[m];
+    // unit prologue: block records and halo record heads (cp.async, completed
+    // with the first tile's group), the halo list and the velocity tables
+    {
+      const uint4* src = reinterpret_cast<const uint4*>(a.rec + e0);
+      for (int w = tid; w < nb * RW; w += NT) cp_async16(reinterpret_cast<uint4*>(recs) + w, src + w);
+      const int* __restrict__ hlist = a.halo_list + h0;
+      for (int w = tid; w < nh * HW; w += NT) {
+        const int s = w / HW, k = w - s * HW;
+        cp_async16(hrec + (size_t)s * HR + 16 * k, reinterpret_cast<const uint4*>(a.rec + hlist[s]) + k);
+      }
+      for (int s = tid; s < nh; s += NT) hl[s] = hlist[s];
+      const int v0 = vt0 * VT;
+      for (int v = tid; v < ntl * VT; v += NT) {
+        vtab[v] = a.cx[v0 + v];
+        vtab[UV + v] = a.cy[v0 + v];
+        vtab[2 * UV + v] = a.nfinf[v0 + v];
       }
     }
-    for (int h = ty; ok && h < nh; h += TY) {
-      const ElemRec<T>& r = *reinterpret_cast<const ElemRec<T>*>(halr + (size_t)h * HB);
-      const int j = EB + h;
-      const T f[3] = {fs[(j * 3 + 0) * VT + tx], fs[(j * 3 + 1) * VT + tx], fs[(j * 3 + 2) * VT + tx]};
-      T qq[3];
-#pragma unroll
-      for (int i = 0; i < 3; ++i) qq[i] = feq_of(r, i, cx, cy);
-      um_s[j * VT + tx] = umean_of(f, qq, r, cx, cy, dth);
-    }
-    __syncthreads();
+    // the rows of tile vt: work item (s, i, half) copies 32 contiguous bytes
+    // of row i of block element s (s < nb, slot s) or halo element s - nb
+    // (slot EB + s - nb)
+    auto issue = [&](int vt, unsigned char* dst) {
+      const T* src = a.fin + (size_t)vt * VT;
+      for (int w = tid; w < n * 6; w += NT) {
+        const int s = w / 6, r = w - 6 * s, i = r >> 1, hf = r & 1;
+        const bool own = s < nb;
+        const int e = own ? e0 + s : hl[s - nb];
+        const int slot = own ? s : EB + (s - nb);
+        const T* g = src + ((size_t)e * 3 + i) * a.Vp + hf * 2 * W;
+        unsigned char* d = dst + (size_t)slot * ER + i * 64 + hf * 32;
+        cp_async16(d, g);
+        cp_async16(d + 16, g + W);
+      }
+    };
+    __syncthreads();  // hl
+    issue(vt0, sm_raw);
+    cp_async_commit();
 
-    // phase 2: volume + edge terms, increment, positivity, inflow reset
-    T rmt = (T)0, sqt = (T)0;
+    for (int k = 0; k < ntl; ++k) {
+      unsigned char* const tl = sm_raw + (size_t)(k & 1) * tile_bytes;
+      cp_async_wait<0>();
+      // tile k has landed for every thread, and every thread is past phase 2
+      // of tile k - 1, whose buffer the next copies overwrite
+      __syncthreads();
+      if (k + 1 < ntl) {
+        issue(vt0 + k + 1, sm_raw + (size_t)((k + 1) & 1) * tile_bytes);
+        cp_async_commit();
+      }
+      const int vb0 = (vt0 + k) * VT;
+      const T* vx = vtab + k * VT;
+      const T* vy = vtab + UV + k * VT;
+      const T* vn = vtab + 2 * UV + k * VT;
+
+      // ---- phase 1: block element j (half hh), then the halo chunk by chunk
+      VecT qr[2][3], ur[2];
+      if (j < nb) {
+        const ElemRec<T>& r = recs[j];
 #pragma unroll
-    for (int m = 0; m < M; ++m) {
-      const int j = ty + TY * m;
-      if (ok && j < nb && vok) {
+        for (int cc = 0; cc < 2; ++cc) {
+          const int c = 2 * hh + cc;
+          sweep_p1<T>(r, tl + (size_t)j * ER + 16 * c, vld<T>(vx + c * W), vld<T>(vy + c * W), dth, dth3, qr[cc],
+                      ur[cc]);
+        }
+      }
+      for (int w = tid; w < nh * NCH; w += NT) {
+        const int hs = w >> 2, c = w & 3;
+        const ElemRec<T>& r = *reinterpret_cast<const ElemRec<T>*>(hrec + (size_t)hs * HR);
+        VecT qd[3], ud;
+        sweep_p1<T>(r, tl + (size_t)(EB + hs) * ER + 16 * c, vld<T>(vx + c * W), vld<T>(vy + c * W), dth, dth3, qd,
+                    ud);
+      }
+      __syncthreads();
+
+      // ---- phase 2: the update of block element j, half hh
+      T rmt = (T)0, sqt = (T)0;
+      if (j < nb) {
+        const ElemRec<T>& r = recs[j];
         const int e = e0 + j;
-        const ElemRec<T>& r = recs[j];
-        const T u = um[m];
-        const T f[3] = {fs[(j * 3 + 0) * VT + tx], fs[(j * 3 + 1) * VT + tx], fs[(j * 3 + 2) * VT + tx]};
-        // GETELC second half: RHS_i = AREA*(N_i,x FXME + N_i,y FYME)
-        const T fm = ((f[0] - u) + (f[1] - u) + (f[2] - u)) * (T)(1.0 / 3.0);
-        const T afm = r.area * fm;
-        T rhs[3];
-#pragma unroll
-        for (int i = 0; i < 3; ++i) rhs[i] = sv[m][i] * afm;
-        // EDGFLXOPT / GETBOU, gathered per element
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-          const int p = k, qn = (k + 1) % 3;
-          const ElemEdge<T> ed = r.edge[k];
-          const int kind = ed.info & 3;
-          if (kind == 1) continue;  // inflow sides carry no flux
-          const T sc = ed.nx * cx + ed.ny * cy;
-          T up, uq;
-          if (kind == 0) {
-            // upwind values without divergence: read the own or the
-            // neighbour's rows of the tile, whichever is upwind
-            const bool left = (ed.info & 4) != 0;
-            const bool mine = left ? (sc > (T)0) : (sc >= (T)0);
-            const int sl = mine ? j : (ed.info >> 8);
-            const int rp = mine ? p : ((ed.info >> 3) & 3), rq = mine ? qn : ((ed.info >> 5) & 3);
-            const T un = mine ? u : um_s[sl * VT + tx];
-            up = fs[(sl * 3 + rp) * VT + tx] - un;
-            uq = fs[(sl * 3 + rq) * VT + tx] - un;
-          } else if (kind == 2 || sc >= (T)0) {
-            up = f[p] - u;
-            uq = f[qn] - u;
-          } else {
-            // wall, molecules leaving the wall (src/getbou.f90:189-255): the
-            // fully diffuse part ALPHA*ETA*Mw (ALPHA < 1 is not built)
-            const int bs = ed.info >> 8;
-            const T tw = a.bTw[bs];
-            const T uwx = a.bUw[2 * bs], uwy = a.bUw[2 * bs + 1];
-            T mw;
-            if (uwx == (T)0 && uwy == (T)0) {
-              const T spd = sqrt(cx * cx + cy * cy);
-              mw = dexp<T>(-(spd * spd) / ((T)2 * a.rgas * tw));
-            } else {
-              const T dx = cx - uwx, dy = cy - uwy;
-              mw = dexp<T>(-(dx * dx + dy * dy) / ((T)2 * a.rgas * tw));
-            }
-            up = uq = a.alpha * (mw * a.bEta[bs]);
-          }
-          const T fnp = sc * up, fnq = sc * uq;
-          rhs[p] -= ed.alen * ((T)2 * fnp + fnq);
-          rhs[qn] -= ed.alen * (fnp + (T)2 * fnq);
-        }
-        // GETINC / CMMINC, ADTHEM, INFLOW
-        T sq = (T)0, rm = (T)0;
+        const unsigned char* own = tl + (size_t)j * ER;
+        const T area3 = r.area * third;
+        T mudt[3], mmdt[3], cmx[3], cmn[3];
 #pragma unroll
         for (int i = 0; i < 3; ++i) {
-          const T x = rhs[i] * dt;
-          const T cdt = r.mu[i] * (q[m][i] - f[i]) * dt;
-          const T d = r.mm[i] * x + cdt;
-          T rr;
-          if (a.immat == 1) {
-            rr = fabs(d);
-          } else {
-            const T c = (x >= (T)0) ? a.cmax[3 * e + i] : a.cmin[3 * e + i];
-            rr = c * x + cdt;
-            rr = rr > (T)0 ? rr : (T)0;
+          mudt[i] = r.mu[i] * dt;
+          mmdt[i] = r.mm[i] * dt;
+          if (IMMAT == 0) {
+            cmx[i] = a.cmax[3 * e + i];
+            cmn[i] = a.cmin[3 * e + i];
           }
-          rm = rr > rm ? rr : rm;
-          sq += d * d;
-          T fn = f[i] + d;
-          if (fn < (T)0) fn = (T)0;
-          if (r.inflow & (1 << i)) fn = a.nfinf[v];
-          __stcs(a.fout + ((size_t)e * 3 + i) * a.Vp + v, fn);
         }
-        rmt = rm > rmt ? rm : rmt;
-        sqt += sq;
+        // per edge: the flux source's rows and AL*n (zero on inflow and
+        // wall sides, whose flux the wall path adds)
+        const unsigned char* srcp[3];
+        const unsigned char* srcq[3];
+        T anx[3], any[3];
+#pragma unroll
+        for (int k2 = 0; k2 < 3; ++k2) {
+          const int inf = r.edge[k2].info, kind = inf & 3;
+          const unsigned char* sb = tl + (size_t)(inf >> 8) * ER;
+          srcp[k2] = sb + ((inf >> 3) & 3) * 64;
+          srcq[k2] = sb + ((inf >> 5) & 3) * 64;
+          const T al = (kind == 0 || kind == 2) ? r.edge[k2].alen : (T)0;
+          anx[k2] = al * r.edge[k2].nx;
+          any[k2] = al * r.edge[k2].ny;
+        }
+        const int flags = r.flags;
+#pragma unroll
+        for (int cc = 0; cc < 2; ++cc) {
+          const int c = 2 * hh + cc;
+          const int vb = vb0 + c * W;
+          if (vb >= a.V) break;
+          const VecT cxv = vld<T>(vx + c * W), cyv = vld<T>(vy + c * W);
+          VecT g[3];
+#pragma unroll
+          for (int i = 0; i < 3; ++i) g[i] = vld<T>(own + 64 * i + 16 * c);
+          // GETELC second half: RHS_i = AREA*(N_i,x FXME + N_i,y FYME), FXME
+          // = cx * mean(g), FYME = cy * mean(g); the P1 gradients sum to
+          // zero, so RHS_3 = -(RHS_1 + RHS_2)
+          T rhs[3][W];
+#pragma unroll
+          for (int w = 0; w < W; ++w) {
+            const T cx = VO::get(cxv, w), cy = VO::get(cyv, w);
+            const T s3 = (VO::get(g[0], w) + VO::get(g[1], w) + VO::get(g[2], w)) * area3;
+            rhs[0][w] = (r.gx[0] * cx + r.gy[0] * cy) * s3;
+            rhs[1][w] = (r.gx[1] * cx + r.gy[1] * cy) * s3;
+            rhs[2][w] = -(rhs[0][w] + rhs[1][w]);
+          }
+          // edge fluxes: RHS_p -= AL*SC*(2 u_p + u_q), RHS_q -= AL*SC*(u_p + 2 u_q)
+#pragma unroll
+          for (int k2 = 0; k2 < 3; ++k2) {
+            const int p = k2, qn = (k2 + 1) % 3;
+            const VecT gp = vld<T>(srcp[k2] + 16 * c), gq = vld<T>(srcq[k2] + 16 * c);
+#pragma unroll
+            for (int w = 0; w < W; ++w) {
+              const T as = anx[k2] * VO::get(cxv, w) + any[k2] * VO::get(cyv, w);
+              const bool mine = as > (T)0;
+              const T up = mine ? VO::get(g[p], w) : VO::get(gp, w);
+              const T uq = mine ? VO::get(g[qn], w) : VO::get(gq, w);
+              rhs[p][w] -= as * ((T)2 * up + uq);
+              rhs[qn][w] -= as * (up + (T)2 * uq);
+            }
+          }
+          if (flags & 0x38) {
+            // wall sides; molecules leaving the wall (src/getbou.f90:189-255)
+            // carry the fully diffuse part ALPHA*ETA*Mw (ALPHA < 1 is not built)
+#pragma unroll
+            for (int k2 = 0; k2 < 3; ++k2) {
+              if (!(flags & (8 << k2))) continue;
+              const int p = k2, qn = (k2 + 1) % 3;
+              const int bs = r.bside[k2];
+              const T twr = (T)2 * a.rgas * a.bTw[bs];
+              const T uwx = a.bUw[2 * bs], uwy = a.bUw[2 * bs + 1], eta = a.bEta[bs];
+              const T nx = r.edge[k2].nx, ny = r.edge[k2].ny, alw = r.edge[k2].alen;
+#pragma unroll
+              for (int w = 0; w < W; ++w) {
+                const T cx = VO::get(cxv, w), cy = VO::get(cyv, w);
+                const T sc = nx * cx + ny * cy;
+                T up, uq;
+                if (sc >= (T)0) {
+                  up = VO::get(g[p], w);
+                  uq = VO::get(g[qn], w);
+                } else {
+                  T mw;
+                  if (uwx == (T)0 && uwy == (T)0) {
+                    const T spd = sqrt(cx * cx + cy * cy);
+                    mw = dexp<T>(-(spd * spd) / twr);
+                  } else {
+                    const T dx = cx - uwx, dy = cy - uwy;
+                    mw = dexp<T>(-(dx * dx + dy * dy) / twr);
+                  }
+                  up = uq = a.alpha * (mw * eta);
+                }
+                const T as = alw * sc;
+                rhs[p][w] -= as * ((T)2 * up + uq);
+                rhs[qn][w] -= as * (up + (T)2 * uq);
+              }
+            }
+          }
+          // GETINC / CMMINC, ADTHEM (f >= 0), INFLOW; the padding past V
+          // stays zero
+          VecT out[3];
+          auto finish = [&](auto full) {
+#pragma unroll
+            for (int w = 0; w < W; ++w) {
+              const bool live = decltype(full)::value || vb + w < a.V;
+              const T u = VO::get(ur[cc], w);
+#pragma unroll
+              for (int i = 0; i < 3; ++i) {
+                const T f = VO::get(g[i], w) + u;
+                const T qmf = VO::get(qr[cc][i], w) - f;
+                T d, rr;
+                if (IMMAT == 1) {
+                  d = mmdt[i] * rhs[i][w] + mudt[i] * qmf;
+                  rr = fabs(d);
+                } else {
+                  const T x = rhs[i][w] * dt, cdt = mudt[i] * qmf;
+                  d = r.mm[i] * x + cdt;
+                  rr = ((x >= (T)0) ? cmx[i] : cmn[i]) * x + cdt;
+                  rr = rr > (T)0 ? rr : (T)0;
+                }
+                T fn = f + d;
+                fn = fn > (T)0 ? fn : (T)0;
+                if (live) {
+                  rmt = rr > rmt ? rr : rmt;
+                  sqt += d * d;
+                } else {
+                  fn = (T)0;
+                }
+                VO::set(out[i], w, fn);
+              }
+            }
+          };
+          if (vb + W <= a.V)
+            finish(std::true_type());
+          else
+            finish(std::false_type());
+          if (flags & 7) {
+            const VecT nf = vld<T>(vn + c * W);  // zero past V
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+              if (flags & (1 << i)) out[i] = nf;
+          }
+#pragma unroll
+          for (int i = 0; i < 3; ++i)
+            __stcs(reinterpret_cast<VecT*>(a.fout + ((size_t)e * 3 + i) * a.Vp + vb), out[i]);
+        }
       }
+      rmax = fmax(rmax, (double)rmt);
+      rsq += (double)sqt;
     }
-    rmax = fmax(rmax, (double)rmt);
-    rsq += (double)sqt;
-    // stage s and um_s are free; all threads learn whether any wait expired
-    if (__syncthreads_or(ok ? 0 : 1)) {
-      aborted = true;
-      break;
-    }
-    if (ty == 0 && t + 2 * G < ntiles) {
-      if (tx == 0) fence_proxy_async_smem();
-      __syncwarp();
-      issue(t + 2 * G, s);
-    }
-    s ^= 1;
+    // every thread is past phase 2 of the unit's last tile: the records,
+    // tables and halo list may be replaced
+    if (tid == 0) s_unit = next;
+    __syncthreads();
+    unit = s_unit;
+    if (tid == 0 && unit < nunits) next = (int)gridDim.x + atomicAdd(&a.ctrl->sweep_next, 1);
   }
-  if (aborted) {
-    // drain this CTA's copies in flight (bounded) before leaving
-    if (tx == 0 && ty == 0) {
-      a.ctrl->timeout = 1;
-      mbar_wait_bounded(&bars[0], par & 1);
-      mbar_wait_bounded(&bars[1], (par >> 1) & 1);
-    }
-    return;
-  }
-  // per-CTA residual partials (deterministic final reduction in k_resid)
+  // per-CTA residual partials, reduced by k_resid (the sum of squares can
+  // differ in its last bits between runs: which units a CTA draws varies)
   rmax = warp_max(rmax);
   rsq = warp_sum(rsq);
-  if (tx == 0) {
-    red_m[ty] = rmax;
-    red_s[ty] = rsq;
+  if ((tid & 31) == 0) {
+    red_m[tid >> 5] = rmax;
+    red_s[tid >> 5] = rsq;
   }
   __syncthreads();
-  if (tx == 0 && ty == 0) {
+  if (tid == 0) {
     double mm = 0, ss = 0;
-    for (int w = 0; w < TY; ++w) {
+    for (int w = 0; w < NW; ++w) {
       mm = fmax(mm, red_m[w]);
       ss += red_s[w];
     }
@@ -689,6 +851,7 @@ __global__ void __launch_bounds__(1024) k_resid(ResidArgs a) {
     }
     if (c->timeout) c->done = 1;
     if (c->ref == 0.0 && l2 > 0.0) c->ref = l2;
+    c->sweep_next = 0;
     c->step = st + 1;
     if (c->step >= c->max_steps) c->done = 1;
     if (c->tol > 0.0 && l2 <= c->tol * c->ref) c->done = 1;

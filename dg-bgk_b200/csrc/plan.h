@@ -52,11 +52,16 @@ struct Plan {
   std::vector<double> node_ae;         // GEOME(7) of its element
 };
 
-// Device edge word: low bits | (slot or boundary side) << 8.
-inline int edge_info(const Plan& pl, size_t i) {
+// Device edge word of edge i = 3*e + k (ElemEdge::info): the kind, the
+// flux source's local nodes and its tile slot -- the neighbour across an
+// interior side, the element itself (slot own_slot, nodes k and k+1) on a
+// boundary side.
+inline int edge_info(const Plan& pl, size_t i, int own_slot) {
   const PlanEdge& e = pl.edge[i];
-  const int hi = ((e.low & 3) == 0) ? pl.eslot[i] : e.bside;
-  return e.low | (hi << 8);
+  const int kind = e.low & 3;
+  if (kind == 0) return (e.low & ~4) | (pl.eslot[i] << 8);
+  const int k = (int)(i % 3);
+  return kind | (k << 3) | (((k + 1) % 3) << 5) | (own_slot << 8);
 }
 
 // Builds the plan; returns 0 or a DGBGK_E* code with the message in *err.

@@ -3,12 +3,10 @@
 // HBM layout of the distribution function: f[(e*3 + i)*Vp + v] -- element e
 // (in the plan's locality order), DG node i (0..2), discrete velocity v
 // fastest, rows padded to a pitch Vp (a multiple of 32 velocities, so every
-// row starts on a 128-byte boundary and every TMA box coordinate
-// v0 = 32*k is 16-byte aligned).  The padding velocities hold zeros forever
-// (the buffers are cleared at allocation and no kernel writes v >= V), so
-// kernels may read whole 16-byte vectors past V without bounds checks.  A
-// warp reading 32 consecutive velocities of one node issues one fully
-// coalesced 128-byte (FP32) or 256-byte (FP64) request.  Two such buffers are
+// row starts on a 128-byte boundary and splits into whole 64-byte sweep
+// segments).  The padding velocities hold zeros forever (the buffers are
+// cleared at allocation and the kernels write zeros there), so kernels may
+// read whole 16-byte vectors past V without bounds checks.  Two such buffers are
 // kept (ping-pong): within one pseudo-time step the reference updates every
 // element of velocity IV only after all edge fluxes of IV are formed
 // (src/advnce.f90:321-367), i.e. a Jacobi update in space, so the sweep reads
@@ -18,15 +16,16 @@
 
 namespace dgbgk {
 
-constexpr int VTILE = 32;  // velocities per sweep tile (one warp's lanes)
-
 // Per element and local edge k (from local node k to node (k+1) mod 3).
-// info bits: [0,2) kind -- 0 interior side, 1 inflow side (no flux),
-// 2 outflow side, 3 wall side (any other BSIDO type); bit 2: this element is
-// ISIDE(3) (the "left" one); [3,5) neighbour's local node at my point k;
-// [5,7) at my point k+1; [8,32) the neighbour's shared-memory slot in the
-// sweep tile (interior sides) or the boundary side index in BSIDO order
-// (kinds 1..3).
+// The sweep forms every edge flux from an upwind "source" row set: the
+// neighbour across an interior side, the element itself on an outflow side
+// (the upwind value of an outflow side is always the element's own) and, as a
+// placeholder with zero length, on inflow sides (no flux) and wall sides
+// (whose flux the wall path adds).  info bits: [0,2) kind -- 0 interior side,
+// 1 inflow side, 2 outflow side, 3 wall side (any other BSIDO type);
+// [3,5) the source's local node at my point k; [5,7) at my point k+1;
+// [8,32) the source's slot in the sweep tile (block element j: slot j; halo
+// element h: slot EB + h).
 template <class T> struct alignas(16) ElemEdge {
   T nx, ny;   // outward unit normal of this element on this edge
   T alen;     // EL/6 (interior) or RSIDO(3)/6 (boundary)
@@ -34,26 +33,27 @@ template <class T> struct alignas(16) ElemEdge {
 };
 
 // Everything the sweep needs about one element, in one 16-byte-aligned
-// record that a bulk copy brings into shared memory.  The leading "UMEAN
-// part" (shape-function gradients and the GTEQNF / COMPMU parameters of the
-// three DG nodes) is all a halo element needs; the moment kernel rewrites the
-// node parameters every step.
+// record.  The leading part (shape-function gradients and the GTEQNF /
+// COMPMU parameters of the three DG nodes, 21 values) is all a halo element
+// needs; the moment kernel rewrites the node parameters every step.
 template <class T> struct alignas(16) ElemRec {
   T gx[3], gy[3];  // shape-function gradients GEOME(1:3), GEOME(4:6)
   T A[3];    // DISND*BETA2/PI   (0 where DISPS < 1e-20: NFO = 0, src/gteqnf.f90:321)
-  T B[3];    // BETA2 = RHO/(2*PS)
+  T ex[3];   // exponent coefficient of NFO: -BETA2 (FP64), -BETA2*log2(e) (FP32, for 2^x)
   T ux[3];   // DISUX
   T uy[3];   // DISUY
   T mu[3];   // collision frequency MU (src/compmu.f90:284-285)
   T area;    // 0.5 * GEOME(7)   (src/getelc.f90:44)
   T mm[3];   // MMAT (IMMAT = 1) or CMMAT row sums (IMMAT = 0)
-  T pad0[3];
+  int bside[3];  // boundary side index of each wall edge (kind 3), else -1
   ElemEdge<T> edge[3];
-  int inflow;  // bit i: DG node i sits on an inflow-side node (INFLOW)
+  int flags;  // bits [0,3): DG node i sits on an inflow-side node (INFLOW);
+              // bits [3,6): edge k is a wall side
   int pad1[3];
 };
-// bytes of the UMEAN part, rounded up to the 16-byte bulk-copy granule
-template <class T> constexpr unsigned umean_part_bytes() { return (unsigned)((22 * sizeof(T) + 15) / 16 * 16); }
+static_assert(sizeof(ElemRec<float>) == 176 && sizeof(ElemRec<double>) == 336, "record layout");
+// values of the leading part a halo element needs (gx .. mu)
+constexpr int REC_HEAD_VALUES = 21;
 
 // One type-4 wall side for the wall-flux kernel (FLUCON2).
 struct WallSide {
@@ -76,6 +76,7 @@ struct Ctrl {
   double dtc;     // Courant limit DTEc (src/alotim.f90)
   int nparts;     // sweep CTAs writing residual partials
   int timeout;    // set when a bounded device wait gave up
+  int sweep_next; // sweep work units handed out beyond the first wave (reset by k_resid)
 };
 
 }  // namespace dgbgk

@@ -1,6 +1,8 @@
 // C ABI of the DG-BGK sweep on B200 (sm_100a): handle management, device
 // memory, the captured two-step CUDA graph and the state transfers.
+#include <cuda.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <cmath>
@@ -55,6 +57,18 @@ template <class X> void dfree(X*& p) {
   p = nullptr;
 }
 
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    cudaDriverEntryPointQueryResult q;
+    void* p = nullptr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+  }
+  return fn;
+}
+
 struct ImplBase {
   virtual ~ImplBase() {}
   virtual int set_state(const void* src, bool f32) = 0;
@@ -86,6 +100,7 @@ template <class T> struct Impl : ImplBase {
   int Vp = 0;
   // device arrays
   T* f[2] = {nullptr, nullptr};
+  CUtensorMap tm[2];  // f[b] as a 2-D tensor of rows (sweep tile boxes)
   ElemRec<T>* rec = nullptr;
   int *halo_off = nullptr, *halo_list = nullptr;
   T *cmax = nullptr, *cmin = nullptr;
@@ -259,7 +274,31 @@ template <class T> struct Impl : ImplBase {
     return 0;
   }
 
-  using SweepFn = void (*)(SweepArgs<T>);
+  // f[b] as a [3E rows][Vp] tensor; box = one 64-byte velocity segment of
+  // BOX_ROWS rows, 64-byte swizzle (the sweep's tile layout)
+  int make_tensor_maps() {
+    auto enc = tensor_map_encoder();
+    if (!enc) {
+      set_error("cuTensorMapEncodeTiled is not available from the driver");
+      return DGBGK_ECUDA;
+    }
+    const CUtensorMapDataType dt = sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    cuuint64_t dims[2] = {(cuuint64_t)Vp, (cuuint64_t)3 * pl.E};
+    cuuint64_t strides[1] = {(cuuint64_t)Vp * sizeof(T)};
+    cuuint32_t box[2] = {(cuuint32_t)SweepGeo<T>::VT, (cuuint32_t)SweepGeo<T>::BOX_ROWS};
+    cuuint32_t estr[2] = {1, 1};
+    for (int b = 0; b < 2; ++b) {
+      CUresult r = enc(&tm[b], dt, 2, f[b], dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                       CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      if (r != CUDA_SUCCESS) {
+        set_error("cuTensorMapEncodeTiled failed for the state buffer");
+        return DGBGK_ECUDA;
+      }
+    }
+    return 0;
+  }
+
+  using SweepFn = void (*)(const CUtensorMap, const CUtensorMap, SweepArgs<T>);
   SweepFn sweep_fn() const {
     if (pl.EB == 64) return pl.immat == 1 ? k_sweep<T, 64, 1> : k_sweep<T, 64, 0>;
     return pl.immat == 1 ? k_sweep<T, 128, 1> : k_sweep<T, 128, 0>;
@@ -309,6 +348,7 @@ template <class T> struct Impl : ImplBase {
       set_error("sweep tile needs more than 227 KB of shared memory");
       return DGBGK_EUNSUP;
     }
+    TRY(make_tensor_maps());
     SweepFn fn = sweep_fn();
     CK(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sweep_smem()));
     int per_sm = 0;
@@ -409,7 +449,7 @@ template <class T> struct Impl : ImplBase {
     a.tpu = tpu;
     a.alpha = (T)pl.alpha;
     a.rgas = (T)pl.rgas;
-    sweep_fn()<<<sweep_grid, 2 * pl.EB, sweep_smem(), st>>>(a);
+    sweep_fn()<<<sweep_grid, 2 * pl.EB, sweep_smem(), st>>>(tm[src], tm[1 - src], a);
     CK(cudaGetLastError());
     return 0;
   }

@@ -14,15 +14,17 @@
 //               src/advnce.f90:286-377) on tiles of (element block x one
 //               64-byte velocity segment).  Persistent CTAs draw work units
 //               (a block at several tiles); the block's records are staged
-//               once per unit, the tiles' f rows (block and halo) arrive by
-//               double-buffered cp.async copies, and each thread works on
-//               whole elements at 8 (FP32) or 4 (FP64) velocities.
+//               once per unit, the tiles' f rows arrive double-buffered (the
+//               block's as 2-D TMA boxes, the halo's by cp.async), and each
+//               thread works on whole elements at 8 (FP32) or 4 (FP64)
+//               velocities.
 //   k_resid   : GETRES + the residual bookkeeping (src/advnce.f90:385,
 //               422-429), the convergence test and the step counter.
 // Every device-side wait on an mbarrier is bounded: on expiry the kernel
 // sets Ctrl::timeout, drains its own copies with a second bounded wait and
 // returns; the host reports DGBGK_ECUDA.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <type_traits>
@@ -373,29 +375,61 @@ __device__ __forceinline__ double step_dt(const Ctrl* c) {
 
 // Sweep tile geometry.  A tile is one 64-byte segment of velocities (16 FP32
 // or 8 FP64 values) of the three rows of every element of a block and of its
-// halo.  In shared memory an element's three 64-byte row segments sit at an
-// element pitch of 208 bytes, an odd number of 16-byte units, so eight
-// threads that each read their own element's rows with 16-byte vectors fall
-// on eight distinct bank groups.  A work unit is one block at `tpu`
-// consecutive velocity tiles: the block's element records and the halo's
-// record heads are staged in shared memory once per unit, the f rows once
-// per tile (double-buffered).
+// halo: row r = 3*slot + i (block element j: slot j; halo element h: slot
+// EB + h), 64 bytes per row, with the 16-byte chunks of a row permuted by the
+// 64-byte swizzle (chunk c of row r at 16*(c ^ ((r >> 1) & 3))).  The block's
+// rows arrive as 2-D TMA boxes that apply this swizzle, the halo rows by
+// cp.async copies that apply it by hand; with it, eight threads that each
+// read their own element's row with 16-byte vectors fall on eight distinct
+// bank groups.  A work unit is one block at `tpu` consecutive velocity
+// tiles: the block's element records and the halo's record heads are staged
+// in shared memory once per unit, the f rows once per tile (double-buffered).
 template <class T> struct SweepGeo {
   static constexpr int W = 16 / (int)sizeof(T);  // values per 16-byte vector
   static constexpr int VT = 64 / (int)sizeof(T);  // velocities per tile
   static constexpr int NCH = 4;                   // 16-byte chunks per row segment
-  static constexpr int ER = 208;                  // element pitch of a tile (bytes)
+  static constexpr int BOX_ROWS = 192;            // rows of one TMA box
   static constexpr int RW = (int)(sizeof(ElemRec<T>) / 16);                    // record words
   static constexpr int HW = (REC_HEAD_VALUES * (int)sizeof(T) + 15) / 16;        // head words
   static constexpr int HR = 16 * (HW | 1);  // halo head pitch (odd number of words)
   static constexpr int TPU_MAX = 16;
-  // two tiles [EB + max_halo][ER], records [EB], halo heads [max_halo][HR],
+  // one tile buffer, 1024-byte aligned
+  static constexpr size_t tile_bytes(int EB, int max_halo) {
+    return ((size_t)3 * (EB + max_halo) * 64 + 1023) / 1024 * 1024;
+  }
+  // alignment slack, two tiles, records [EB], halo heads [max_halo][HR],
   // velocity tables cx, cy, NFINF [3][TPU_MAX * VT], halo element list
   static constexpr size_t smem(int EB, int max_halo) {
-    return 2 * (size_t)(EB + max_halo) * ER + (size_t)EB * sizeof(ElemRec<T>) + (size_t)max_halo * HR +
+    return 1024 + 2 * tile_bytes(EB, max_halo) + (size_t)EB * sizeof(ElemRec<T>) + (size_t)max_halo * HR +
            3 * (size_t)TPU_MAX * VT * sizeof(T) + ((size_t)max_halo * 4 + 15) / 16 * 16;
   }
 };
+
+// Byte offset of 16-byte chunk c of row r in a tile.
+__device__ __forceinline__ unsigned tile_off(int r, int c) {
+  return (unsigned)(r * 64 + 16 * (c ^ ((r >> 1) & 3)));
+}
+
+// 2-D tiled TMA load (no multicast) of one box into shared memory.
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
+          "r"(smem_u32(dst)),
+      "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+// 2-D tiled TMA store of one box from shared memory (elements outside the
+// tensor are not written), tracked by the issuing thread's bulk groups.
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap* map, int x, int y, const void* src) {
+  asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.tile.bulk_group [%0, {%1, %2}], [%3];" ::"l"(map), "r"(x),
+               "r"(y), "r"(smem_u32(src))
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// the issuing thread's bulk stores have finished reading shared memory
+__device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+// ... and their writes are complete
+__device__ __forceinline__ void bulk_wait0() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 
 // 16-byte asynchronous copy global -> shared through L2 only (cp.async.cg).
 __device__ __forceinline__ void cp_async16(void* dst, const void* src) {
@@ -451,22 +485,26 @@ template <class T> __device__ __forceinline__ void vst(void* p, const typename V
   *reinterpret_cast<typename Vec<T>::type*>(p) = v;
 }
 
-// Phase 1 of the sweep on one 16-byte chunk of an element's three rows in
-// the tile: NFO (GTEQNF, src/gteqnf.f90:324-326) and UMEAN =
+// Phase 1 of the sweep on chunk c of an element's three rows (tile rows
+// r0 .. r0+2): NFO (GTEQNF, src/gteqnf.f90:324-326) and UMEAN =
 // 0.5*DTE*(div F - 1/3 sum_i MU_i (NFO_i - f_i)) with div F = sum_i
 // (N_i,x cx + N_i,y cy) f_i (GETELC, src/getelc.f90:54-83).  The rows are
 // overwritten in place with g = f - UMEAN, the value every edge flux and the
 // volume term of this element use (src/getelc.f90:87-117,
 // src/edgflxopt.f90:95-125); NFO and UMEAN are returned.
 template <class T>
-__device__ __forceinline__ void sweep_p1(const ElemRec<T>& r, unsigned char* row, const typename Vec<T>::type& cxv,
-                                         const typename Vec<T>::type& cyv, T dth, T dth3,
-                                         typename Vec<T>::type (&q)[3], typename Vec<T>::type& u) {
+__device__ __forceinline__ void sweep_p1(const ElemRec<T>& r, unsigned char* tl, int r0, int c,
+                                         const typename Vec<T>::type& cxv, const typename Vec<T>::type& cyv, T dth,
+                                         T dth3, typename Vec<T>::type (&q)[3], typename Vec<T>::type& u) {
   using VO = Vec<T>;
   constexpr int W = SweepGeo<T>::W;
+  unsigned char* row[3];
   typename VO::type f[3];
 #pragma unroll
-  for (int i = 0; i < 3; ++i) f[i] = vld<T>(row + 64 * i);
+  for (int i = 0; i < 3; ++i) {
+    row[i] = tl + tile_off(r0 + i, c);
+    f[i] = vld<T>(row[i]);
+  }
 #pragma unroll
   for (int w = 0; w < W; ++w) {
     const T cx = VO::get(cxv, w), cy = VO::get(cyv, w);
@@ -487,7 +525,7 @@ __device__ __forceinline__ void sweep_p1(const ElemRec<T>& r, unsigned char* row
     for (int i = 0; i < 3; ++i) VO::set(f[i], w, VO::get(f[i], w) - um);
   }
 #pragma unroll
-  for (int i = 0; i < 3; ++i) vst<T>(row + 64 * i, f[i]);
+  for (int i = 0; i < 3; ++i) vst<T>(row[i], f[i]);
 }
 
 // Persistent sweep kernel: EB block elements, 2*EB threads.  Work units are
@@ -496,9 +534,9 @@ __device__ __forceinline__ void sweep_p1(const ElemRec<T>& r, unsigned char* row
 // running at one moment cover neighbouring blocks at the same velocities and
 // the halo rows they read are L2 hits.  Per unit the block's element records
 // and the halo's record heads are staged in shared memory; per tile the
-// three 64-byte row segments of every block and halo element arrive by
-// 16-byte cp.async copies, double-buffered so the next tile's rows load
-// while this one is computed.  Per tile:
+// block's rows arrive as TMA boxes (completing on an mbarrier, bounded wait)
+// and the halo's rows by cp.async copies, double-buffered so the next tile's
+// rows load while this one is computed.  Per tile:
 //  * phase 1: UMEAN and g = f - UMEAN of every block and halo element; a
 //    block element's NFO and UMEAN stay in the registers of the thread that
 //    updates it;
@@ -512,21 +550,27 @@ __device__ __forceinline__ void sweep_p1(const ElemRec<T>& r, unsigned char* row
 // it where SC > 0 for the ISIDE(3) element and SC >= 0 for the other; the
 // two differ only at SC = 0, where the flux SC*value is zero either way.
 template <class T, int EB, int IMMAT>
-__global__ void __launch_bounds__(2 * EB, sizeof(T) == 4 ? 2 : 1) k_sweep(SweepArgs<T> a) {
+__global__ void __launch_bounds__(2 * EB, sizeof(T) == 4 ? 2 : 1)
+    k_sweep(const __grid_constant__ CUtensorMap tm_in, const __grid_constant__ CUtensorMap tm_out,
+            SweepArgs<T> a) {
   if (a.ctrl->done) return;
   using G = SweepGeo<T>;
   using VO = Vec<T>;
   using VecT = typename VO::type;
-  constexpr int W = G::W, VT = G::VT, NCH = G::NCH, ER = G::ER, RW = G::RW, HW = G::HW, HR = G::HR;
+  constexpr int W = G::W, VT = G::VT, NCH = G::NCH, RW = G::RW, HW = G::HW, HR = G::HR;
   constexpr int NT = 2 * EB, NW = NT / 32;
+  constexpr int NBOX = (3 * EB + G::BOX_ROWS - 1) / G::BOX_ROWS;
+  constexpr unsigned BOX_BYTES = G::BOX_ROWS * 64;
   static_assert(EB % 16 == 0, "whole warps");
   extern __shared__ __align__(128) unsigned char sm_raw[];
   __shared__ int s_unit;
   __shared__ double red_m[NW], red_s[NW];
+  __shared__ uint64_t bars[2];  // TMA completion of tile buffer 0 / 1
   const int tid = threadIdx.x;
-  const int slots = EB + a.max_halo;
-  const size_t tile_bytes = (size_t)slots * ER;
-  ElemRec<T>* const recs = reinterpret_cast<ElemRec<T>*>(sm_raw + 2 * tile_bytes);
+  // tile buffers 1024-byte aligned (the swizzle pattern repeats every 512 B)
+  unsigned char* const base = sm_raw + ((1024u - (smem_u32(sm_raw) & 1023u)) & 1023u);
+  const size_t tile_bytes = G::tile_bytes(EB, a.max_halo);
+  ElemRec<T>* const recs = reinterpret_cast<ElemRec<T>*>(base + 2 * tile_bytes);
   unsigned char* const hrec = reinterpret_cast<unsigned char*>(recs + EB);
   T* const vtab = reinterpret_cast<T*>(hrec + (size_t)a.max_halo * HR);  // cx, cy, NFINF
   constexpr int UV = G::TPU_MAX * VT;
@@ -538,6 +582,15 @@ __global__ void __launch_bounds__(2 * EB, sizeof(T) == 4 ? 2 : 1) k_sweep(SweepA
   const double dtd = step_dt(a.ctrl);
   const T dt = (T)dtd, dth = (T)(0.5 * dtd), dth3 = (T)(0.5 * dtd / 3.0), third = (T)(1.0 / 3.0);
   double rmax = 0.0, rsq = 0.0;
+  if (tid == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  uint32_t par = 0;  // bit b: parity of the next phase of bars[b]
+  bool aborted = false;
+  int abort_buf = 0;
 
   int unit = blockIdx.x;
   // the unit after this one, drawn ahead so the atomic's latency is hidden
@@ -546,7 +599,6 @@ __global__ void __launch_bounds__(2 * EB, sizeof(T) == 4 ? 2 : 1) k_sweep(SweepA
     const int b = unit % a.nblocks, vg = unit / a.nblocks;
     const int e0 = b * EB, nb = min(EB, a.E - e0);
     const int h0 = a.halo_off[b], nh = a.halo_off[b + 1] - h0;
-    const int n = nb + nh;
     const int vt0 = vg * a.tpu, ntl = min(a.tpu, a.nvt - vt0);
 
     // unit prologue: block records and halo record heads (cp.async, completed
@@ -570,33 +622,53 @@ __global__ void __launch_bounds__(2 * EB, sizeof(T) == 4 ? 2 : 1) k_sweep(SweepA
     // the rows of tile vt: work item (s, i, half) copies 32 contiguous bytes
     // of row i of block element s (s < nb, slot s) or halo element s - nb
     // (slot EB + s - nb)
-    auto issue = [&](int vt, unsigned char* dst) {
+    // copies of tile vt into buffer bi: the block's rows (3*e0 ..) as NBOX
+    // TMA boxes issued by thread 0 once the buffer's last box store has
+    // read it (rows past 3E read as zeros), the halo rows by cp.async, four
+    // threads per 64-byte row
+    auto issue = [&](int vt, int bi) {
+      unsigned char* dst = base + (size_t)bi * tile_bytes;
+      if (tid == 0) {
+        bulk_wait_read0();
+        fence_proxy_async_smem();  // the buffer's previous generic accesses
+        mbar_expect_tx(&bars[bi], NBOX * BOX_BYTES);
+#pragma unroll
+        for (int x = 0; x < NBOX; ++x)
+          tma_load_2d(dst + x * BOX_BYTES, &tm_in, vt * VT, 3 * e0 + x * G::BOX_ROWS, &bars[bi]);
+      }
       const T* src = a.fin + (size_t)vt * VT;
-      for (int w = tid; w < n * 6; w += NT) {
-        const int s = w / 6, r = w - 6 * s, i = r >> 1, hf = r & 1;
-        const bool own = s < nb;
-        const int e = own ? e0 + s : hl[s - nb];
-        const int slot = own ? s : EB + (s - nb);
-        const T* g = src + ((size_t)e * 3 + i) * a.Vp + hf * 2 * W;
-        unsigned char* d = dst + (size_t)slot * ER + i * 64 + hf * 32;
-        cp_async16(d, g);
-        cp_async16(d + 16, g + W);
+      for (int w = tid; w < nh * 12; w += NT) {
+        const int h = w / 12, rr = w - 12 * h, i = rr >> 2, c = rr & 3;
+        cp_async16(dst + tile_off(3 * (EB + h) + i, c), src + ((size_t)hl[h] * 3 + i) * a.Vp + c * W);
       }
     };
+    // the new block rows of tile vt (written into buffer bi by every thread,
+    // each followed by a proxy fence, before a barrier) as NBOX box stores
+    // issued by thread 0; rows past 3E are not written
+    auto store = [&](int vt, int bi) {
+      const unsigned char* srcb = base + (size_t)bi * tile_bytes;
+#pragma unroll
+      for (int x = 0; x < NBOX; ++x) tma_store_2d(&tm_out, vt * VT, 3 * e0 + x * G::BOX_ROWS, srcb + x * BOX_BYTES);
+      bulk_commit();
+    };
     __syncthreads();  // hl
-    issue(vt0, sm_raw);
+    issue(vt0, 0);
     cp_async_commit();
 
     for (int k = 0; k < ntl; ++k) {
-      unsigned char* const tl = sm_raw + (size_t)(k & 1) * tile_bytes;
+      const int bi = k & 1;
+      unsigned char* const tl = base + (size_t)bi * tile_bytes;
+      const bool ok = mbar_wait_bounded(&bars[bi], (par >> bi) & 1u);
+      par ^= 1u << bi;
       cp_async_wait<0>();
-      // tile k has landed for every thread, and every thread is past phase 2
-      // of tile k - 1, whose buffer the next copies overwrite
-      __syncthreads();
-      if (k + 1 < ntl) {
-        issue(vt0 + k + 1, sm_raw + (size_t)((k + 1) & 1) * tile_bytes);
-        cp_async_commit();
+      // tile k has landed for every thread (or some wait expired), and every
+      // thread has written and fenced its new rows of tile k - 1
+      if (__syncthreads_or(ok ? 0 : 1)) {
+        aborted = true;
+        abort_buf = bi;
+        break;
       }
+      if (tid == 0 && k > 0) store(vt0 + k - 1, bi ^ 1);
       const int vb0 = (vt0 + k) * VT;
       const T* vx = vtab + k * VT;
       const T* vy = vtab + UV + k * VT;
@@ -609,25 +681,32 @@ __global__ void __launch_bounds__(2 * EB, sizeof(T) == 4 ? 2 : 1) k_sweep(SweepA
 #pragma unroll
         for (int cc = 0; cc < 2; ++cc) {
           const int c = 2 * hh + cc;
-          sweep_p1<T>(r, tl + (size_t)j * ER + 16 * c, vld<T>(vx + c * W), vld<T>(vy + c * W), dth, dth3, qr[cc],
-                      ur[cc]);
+          sweep_p1<T>(r, tl, 3 * j, c, vld<T>(vx + c * W), vld<T>(vy + c * W), dth, dth3, qr[cc], ur[cc]);
         }
       }
       for (int w = tid; w < nh * NCH; w += NT) {
         const int hs = w >> 2, c = w & 3;
         const ElemRec<T>& r = *reinterpret_cast<const ElemRec<T>*>(hrec + (size_t)hs * HR);
         VecT qd[3], ud;
-        sweep_p1<T>(r, tl + (size_t)(EB + hs) * ER + 16 * c, vld<T>(vx + c * W), vld<T>(vy + c * W), dth, dth3, qd,
-                    ud);
+        sweep_p1<T>(r, tl, 3 * (EB + hs), c, vld<T>(vx + c * W), vld<T>(vy + c * W), dth, dth3, qd, ud);
       }
       __syncthreads();
+      // the other buffer's tile k - 1 is stored (or being stored): load tile k + 1
+      if (k + 1 < ntl) {
+        issue(vt0 + k + 1, bi ^ 1);
+        cp_async_commit();
+      }
 
-      // ---- phase 2: the update of block element j, half hh
+      // ---- phase 2: the update of block element j, half hh.  Row offsets
+      // are taken at chunk 2*hh; chunk 2*hh+1 of the same row is at offset ^ 16.
       T rmt = (T)0, sqt = (T)0;
+      unsigned own[3];
+#pragma unroll
+      for (int i = 0; i < 3; ++i) own[i] = tile_off(3 * j + i, 2 * hh);
+      VecT outv[2][3];
       if (j < nb) {
         const ElemRec<T>& r = recs[j];
         const int e = e0 + j;
-        const unsigned char* own = tl + (size_t)j * ER;
         const T area3 = r.area * third;
         T mudt[3], mmdt[3], cmx[3], cmn[3];
 #pragma unroll
@@ -641,15 +720,14 @@ __global__ void __launch_bounds__(2 * EB, sizeof(T) == 4 ? 2 : 1) k_sweep(SweepA
         }
         // per edge: the flux source's rows and AL*n (zero on inflow and
         // wall sides, whose flux the wall path adds)
-        const unsigned char* srcp[3];
-        const unsigned char* srcq[3];
+        unsigned srcp[3], srcq[3];
         T anx[3], any[3];
 #pragma unroll
         for (int k2 = 0; k2 < 3; ++k2) {
           const int inf = r.edge[k2].info, kind = inf & 3;
-          const unsigned char* sb = tl + (size_t)(inf >> 8) * ER;
-          srcp[k2] = sb + ((inf >> 3) & 3) * 64;
-          srcq[k2] = sb + ((inf >> 5) & 3) * 64;
+          const int r0 = 3 * (inf >> 8);
+          srcp[k2] = tile_off(r0 + ((inf >> 3) & 3), 2 * hh);
+          srcq[k2] = tile_off(r0 + ((inf >> 5) & 3), 2 * hh);
           const T al = (kind == 0 || kind == 2) ? r.edge[k2].alen : (T)0;
           anx[k2] = al * r.edge[k2].nx;
           any[k2] = al * r.edge[k2].ny;
@@ -658,12 +736,18 @@ __global__ void __launch_bounds__(2 * EB, sizeof(T) == 4 ? 2 : 1) k_sweep(SweepA
 #pragma unroll
         for (int cc = 0; cc < 2; ++cc) {
           const int c = 2 * hh + cc;
+          const unsigned cx16 = 16u * cc;
           const int vb = vb0 + c * W;
-          if (vb >= a.V) break;
+          VecT(&out)[3] = outv[cc];
+          if (vb >= a.V) {  // all past V: the padding stays zero
+#pragma unroll
+            for (int i = 0; i < 3; ++i) out[i] = VecT{};
+            continue;
+          }
           const VecT cxv = vld<T>(vx + c * W), cyv = vld<T>(vy + c * W);
           VecT g[3];
 #pragma unroll
-          for (int i = 0; i < 3; ++i) g[i] = vld<T>(own + 64 * i + 16 * c);
+          for (int i = 0; i < 3; ++i) g[i] = vld<T>(tl + (own[i] ^ cx16));
           // GETELC second half: RHS_i = AREA*(N_i,x FXME + N_i,y FYME), FXME
           // = cx * mean(g), FYME = cy * mean(g); the P1 gradients sum to
           // zero, so RHS_3 = -(RHS_1 + RHS_2)
@@ -680,7 +764,7 @@ __global__ void __launch_bounds__(2 * EB, sizeof(T) == 4 ? 2 : 1) k_sweep(SweepA
 #pragma unroll
           for (int k2 = 0; k2 < 3; ++k2) {
             const int p = k2, qn = (k2 + 1) % 3;
-            const VecT gp = vld<T>(srcp[k2] + 16 * c), gq = vld<T>(srcq[k2] + 16 * c);
+            const VecT gp = vld<T>(tl + (srcp[k2] ^ cx16)), gq = vld<T>(tl + (srcq[k2] ^ cx16));
 #pragma unroll
             for (int w = 0; w < W; ++w) {
               const T as = anx[k2] * VO::get(cxv, w) + any[k2] * VO::get(cyv, w);
@@ -729,7 +813,6 @@ __global__ void __launch_bounds__(2 * EB, sizeof(T) == 4 ? 2 : 1) k_sweep(SweepA
           }
           // GETINC / CMMINC, ADTHEM (f >= 0), INFLOW; the padding past V
           // stays zero
-          VecT out[3];
           auto finish = [&](auto full) {
 #pragma unroll
             for (int w = 0; w < W; ++w) {
@@ -771,18 +854,38 @@ __global__ void __launch_bounds__(2 * EB, sizeof(T) == 4 ? 2 : 1) k_sweep(SweepA
             for (int i = 0; i < 3; ++i)
               if (flags & (1 << i)) out[i] = nf;
           }
-#pragma unroll
-          for (int i = 0; i < 3; ++i)
-            __stcs(reinterpret_cast<VecT*>(a.fout + ((size_t)e * 3 + i) * a.Vp + vb), out[i]);
         }
       }
       rmax = fmax(rmax, (double)rmt);
       rsq += (double)sqt;
+      // every thread is past its phase-2 reads of tile k: the new rows
+      // replace the block rows in the buffer, for the box store
+      __syncthreads();
+      if (j < nb) {
+#pragma unroll
+        for (int cc = 0; cc < 2; ++cc)
+#pragma unroll
+          for (int i = 0; i < 3; ++i) vst<T>(tl + (own[i] ^ (16u * cc)), outv[cc][i]);
+      }
+      fence_proxy_async_smem();
     }
-    // every thread is past phase 2 of the unit's last tile: the records,
-    // tables and halo list may be replaced
+    if (aborted) {
+      // a bounded wait expired (the vote made every thread leave the tile
+      // loop together): drain this CTA's box copies in flight, bounded, and
+      // report through the control block
+      if (tid == 0) {
+        a.ctrl->timeout = 1;
+        mbar_wait_bounded(&bars[abort_buf], ((par >> abort_buf) & 1u) ^ 1u);
+        bulk_wait0();
+      }
+      return;
+    }
+    // every thread is past phase 2 of the unit's last tile and has written
+    // its rows: store the last tile; the records, tables and halo list may
+    // be replaced
     if (tid == 0) s_unit = next;
     __syncthreads();
+    if (tid == 0) store(vt0 + ntl - 1, (ntl - 1) & 1);
     unit = s_unit;
     if (tid == 0 && unit < nunits) next = (int)gridDim.x + atomicAdd(&a.ctrl->sweep_next, 1);
   }
@@ -803,6 +906,7 @@ __global__ void __launch_bounds__(2 * EB, sizeof(T) == 4 ? 2 : 1) k_sweep(SweepA
     }
     a.part_max[blockIdx.x] = mm;
     a.part_sq[blockIdx.x] = ss;
+    bulk_wait0();  // the last box stores are complete before the CTA exits
   }
 }
 

@@ -115,7 +115,7 @@ template <class T> struct Impl : ImplBase {
   double* node_ae = nullptr;
   double *part_max = nullptr, *part_sq = nullptr;
   int nparts = 0, sweep_grid = 0, part_cap = 0;
-  int mom_grid = 0, mom_warps = 0, mom_stages = 0;
+  int mom_grid = 0, mom_warps = 0, mom_stages = 0, mom_rows = 4;
   size_t mom_smem = 0;
   double *hist_linf = nullptr, *hist_l2 = nullptr, *hist_dt = nullptr;
   int hist_cap = 0;
@@ -241,38 +241,50 @@ template <class T> struct Impl : ImplBase {
 
   // Moment kernel: per-warp rings of velocity rows, persistent grid.  Picks
   // the (warps per CTA, ring stages) with the most resident warps per SM.
+  // Moment kernel: per-warp rings of R-row stages, persistent grid.  Picks
+  // (rows per warp step R, warps per CTA, ring stages) with the most resident
+  // warps per SM, then the most rows in flight, then the fewest rows per warp
+  // step (measured on B200 at 24x48 velocities: one row per warp step was
+  // fastest in FP32 and FP64).
   int config_moments() {
     const size_t rowbytes = ((size_t)pl.V * sizeof(T) + 15) / 16 * 16;
     const size_t tbytes = 3 * (size_t)Vp * sizeof(T);
     const size_t cap = 227 * 1024, sm_total = 228 * 1024;
-    int best = -1;
-    for (int w : {16, 12, 8, 6, 4, 2, 1})
-      for (int sg : {3, 2}) {
-        const size_t bytes = 128 * (((size_t)w * sg * 8 + 127) / 128) + tbytes + (size_t)w * sg * rowbytes;
-        if (bytes > cap) continue;
-        const int blocks = (int)std::min<size_t>(4, sm_total / (bytes + 1024));
-        const int score = blocks * w * 4 + sg;  // resident warps first, then stages
-        if (blocks >= 1 && score > best) {
-          best = score;
-          mom_warps = w;
-          mom_stages = sg;
-          mom_smem = bytes;
+    long best = -1;
+    for (int R : {4, 2, 1})
+      for (int w : {16, 12, 10, 8, 6, 5, 4, 3, 2, 1})
+        for (int sg : {3, 2}) {
+          const size_t bytes =
+              128 * (((size_t)w * sg * 8 + 127) / 128) + tbytes + (size_t)w * sg * R * rowbytes;
+          if (bytes > cap) continue;
+          const int blocks = (int)std::min<size_t>(4, sm_total / (bytes + 1024));
+          if (blocks < 1) continue;
+          const long score = ((long)blocks * w * 1024 + (long)blocks * w * (sg - 1) * R) * 8 + (8 - R);
+          if (score > best) {
+            best = score;
+            mom_rows = R;
+            mom_warps = w;
+            mom_stages = sg;
+            mom_smem = bytes;
+          }
         }
-      }
     if (best < 0) {
       set_error("velocity rows too long for the moment kernel's shared-memory ring");
       return DGBGK_EUNSUP;
     }
     const int warps = mom_warps;
-    CK(cudaFuncSetAttribute(k_moments<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mom_smem));
+    MomFn fn = mom_fn();
+    CK(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mom_smem));
     int per_sm = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_moments<T>, warps * 32, mom_smem));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)fn, warps * 32, mom_smem));
     if (per_sm < 1) per_sm = 1;
-    const int ndg = 3 * pl.E;
-    const int need = (ndg + warps - 1) / warps;
+    const int ngroups = (3 * pl.E + mom_rows - 1) / mom_rows;
+    const int need = (ngroups + warps - 1) / warps;
     mom_grid = std::max(1, std::min(need, per_sm * nsm));
     return 0;
   }
+  using MomFn = void (*)(MomArgs<T>);
+  MomFn mom_fn() const { return mom_rows == 4 ? k_moments<T, 4> : mom_rows == 2 ? k_moments<T, 2> : k_moments<T, 1>; }
 
   // f[b] as a [3E rows][Vp] tensor; box = one 64-byte velocity segment of
   // BOX_ROWS rows, 64-byte swizzle (the sweep's tile layout)
@@ -411,7 +423,7 @@ template <class T> struct Impl : ImplBase {
     a.MM = pl.M / 6.022e26;
     a.sigt = 3.1416 * pl.d * pl.d;
     CK(cudaMemsetAsync(&ctrl->maxmu, 0, sizeof(double), st));
-    k_moments<T><<<mom_grid, mom_warps * 32, mom_smem, st>>>(a);
+    mom_fn()<<<mom_grid, mom_warps * 32, mom_smem, st>>>(a);
     CK(cudaGetLastError());
     return 0;
   }

@@ -3,11 +3,11 @@
 // One step (src/advnce.f90:220-400) is four launches on one stream:
 //   k_moments : MACROS passes 1+2 (src/macros.f90:80-154) fused with COMPMU
 //               (src/compmu.f90:242-290) and the GTEQNF parameters
-//               (src/gteqnf.f90:315-326).  Persistent warps stream whole
-//               velocity rows of f into shared memory with 1-D bulk copies
-//               (cp.async.bulk, a ring of stages per warp), so f is read from
-//               HBM once for both passes; the velocity tables sit in shared
-//               memory and every access is a 16-byte vector.
+//               (src/gteqnf.f90:315-326).  Persistent warps take R whole
+//               velocity rows of f at a time (32/R lanes per row) from a
+//               per-warp ring of stages filled by 1-D bulk copies, so f is
+//               read from HBM once for both passes; the velocity tables sit
+//               in shared memory and every access is a 16-byte vector.
 //   k_wall    : FLUCON2 (src/flucon2.f90:134-233), one warp per wall side.
 //   k_sweep   : the whole velocity-loop body (GTEQNF, GETFLA, GETELC,
 //               EDGFLXOPT/GETBOU, GETINC/CMMINC, ADTHEM, INFLOW;
@@ -137,20 +137,20 @@ __device__ __forceinline__ double sqrt_newton(double x) {
 }
 __device__ __forceinline__ float sqrt_fast(float x) { return x > 0.f ? x * rsqrtf(x) : 0.f; }
 
-// Pass sums over one velocity row in shared memory, one 16-byte vector per
-// lane and iteration.  FP64 storage: FP64 arithmetic.  FP32 storage: FP32
-// products and 4-value partial sums accumulated in FP64 (an FP64-accumulated
-// FP32 kernel was FP64-pipe bound).
+// Pass sums over one velocity row in shared memory by the L lanes of a
+// group (lane sub takes 16-byte vectors sub, sub+L, ...).  FP64 storage:
+// FP64 arithmetic.  FP32 storage: FP32 arithmetic; each lane's partial sums
+// (V/(4L) vectors) are converted to FP64 before the group sum.
 template <class T> struct RowMath;
 
 template <> struct RowMath<double> {
-  static __device__ __forceinline__ void pass1(const double* row, const double* tb, int Vp, int nq, int lane,
+  static __device__ __forceinline__ void pass1(const double* row, const double* tb, int Vp, int nq, int sub, int L,
                                                double& s0, double& s1, double& s2) {
     const double2* r = reinterpret_cast<const double2*>(row);
     const double2* cx = reinterpret_cast<const double2*>(tb);
     const double2* cy = reinterpret_cast<const double2*>(tb + Vp);
     const double2* wj = reinterpret_cast<const double2*>(tb + 2 * Vp);
-    for (int q = lane; q < nq; q += 32) {
+    for (int q = sub; q < nq; q += L) {
       const double2 x = r[q], c = cx[q], d = cy[q], w = wj[q];
       const double a0 = w.x * x.x, a1 = w.y * x.y;
       s0 += a0 + a1;
@@ -158,13 +158,13 @@ template <> struct RowMath<double> {
       s2 = fma(d.x, a0, fma(d.y, a1, s2));
     }
   }
-  static __device__ __forceinline__ void pass2(const double* row, const double* tb, int Vp, int nq, int lane,
+  static __device__ __forceinline__ void pass2(const double* row, const double* tb, int Vp, int nq, int sub, int L,
                                                double ux, double uy, double& sp, double& sc) {
     const double2* r = reinterpret_cast<const double2*>(row);
     const double2* cx = reinterpret_cast<const double2*>(tb);
     const double2* cy = reinterpret_cast<const double2*>(tb + Vp);
     const double2* wj = reinterpret_cast<const double2*>(tb + 2 * Vp);
-    for (int q = lane; q < nq; q += 32) {
+    for (int q = sub; q < nq; q += L) {
       const double2 x = r[q], c = cx[q], d = cy[q], w = wj[q];
       const double dx0 = c.x - ux, dy0 = d.x - uy, dx1 = c.y - ux, dy1 = d.y - uy;
       const double q0 = dx0 * dx0 + dy0 * dy0, q1 = dx1 * dx1 + dy1 * dy1;
@@ -176,71 +176,97 @@ template <> struct RowMath<double> {
 };
 
 template <> struct RowMath<float> {
-  static __device__ __forceinline__ void pass1(const float* row, const float* tb, int Vp, int nq, int lane,
+  static __device__ __forceinline__ void pass1(const float* row, const float* tb, int Vp, int nq, int sub, int L,
                                                double& s0, double& s1, double& s2) {
     const float4* r = reinterpret_cast<const float4*>(row);
     const float4* cx = reinterpret_cast<const float4*>(tb);
     const float4* cy = reinterpret_cast<const float4*>(tb + Vp);
     const float4* wj = reinterpret_cast<const float4*>(tb + 2 * Vp);
-    for (int q = lane; q < nq; q += 32) {
+    float t0 = 0.f, t1 = 0.f, t2 = 0.f;
+    for (int q = sub; q < nq; q += L) {
       const float4 x = r[q], c = cx[q], d = cy[q], w = wj[q];
       const float a0 = w.x * x.x, a1 = w.y * x.y, a2 = w.z * x.z, a3 = w.w * x.w;
-      s0 += (double)((a0 + a1) + (a2 + a3));
-      s1 += (double)fmaf(c.x, a0, fmaf(c.y, a1, fmaf(c.z, a2, c.w * a3)));
-      s2 += (double)fmaf(d.x, a0, fmaf(d.y, a1, fmaf(d.z, a2, d.w * a3)));
+      t0 += (a0 + a1) + (a2 + a3);
+      t1 = fmaf(c.x, a0, fmaf(c.y, a1, fmaf(c.z, a2, fmaf(c.w, a3, t1))));
+      t2 = fmaf(d.x, a0, fmaf(d.y, a1, fmaf(d.z, a2, fmaf(d.w, a3, t2))));
     }
+    s0 += (double)t0;
+    s1 += (double)t1;
+    s2 += (double)t2;
   }
-  static __device__ __forceinline__ void pass2(const float* row, const float* tb, int Vp, int nq, int lane,
+  static __device__ __forceinline__ void pass2(const float* row, const float* tb, int Vp, int nq, int sub, int L,
                                                double ux, double uy, double& sp, double& sc) {
     const float fx = (float)ux, fy = (float)uy;
     const float4* r = reinterpret_cast<const float4*>(row);
     const float4* cx = reinterpret_cast<const float4*>(tb);
     const float4* cy = reinterpret_cast<const float4*>(tb + Vp);
     const float4* wj = reinterpret_cast<const float4*>(tb + 2 * Vp);
-    for (int q = lane; q < nq; q += 32) {
+    float tp = 0.f, tc = 0.f;
+    for (int q = sub; q < nq; q += L) {
       const float4 x = r[q], c = cx[q], d = cy[q], w = wj[q];
       const float e0 = c.x - fx, e1 = c.y - fx, e2 = c.z - fx, e3 = c.w - fx;
       const float g0 = d.x - fy, g1 = d.y - fy, g2 = d.z - fy, g3 = d.w - fy;
       const float q0 = fmaf(e0, e0, g0 * g0), q1 = fmaf(e1, e1, g1 * g1), q2 = fmaf(e2, e2, g2 * g2),
                   q3 = fmaf(e3, e3, g3 * g3);
       const float a0 = w.x * x.x, a1 = w.y * x.y, a2 = w.z * x.z, a3 = w.w * x.w;
-      sp += (double)(0.5f * fmaf(q0, a0, fmaf(q1, a1, fmaf(q2, a2, q3 * a3))));
-      sc += (double)fmaf(sqrt_fast(q0), a0, fmaf(sqrt_fast(q1), a1, fmaf(sqrt_fast(q2), a2, sqrt_fast(q3) * a3)));
+      tp = fmaf(q0, a0, fmaf(q1, a1, fmaf(q2, a2, fmaf(q3, a3, tp))));
+      tc = fmaf(sqrt_fast(q0), a0, fmaf(sqrt_fast(q1), a1, fmaf(sqrt_fast(q2), a2, fmaf(sqrt_fast(q3), a3, tc))));
     }
+    sp += 0.5 * (double)tp;
+    sc += (double)tc;
   }
 };
 
-template <class T>
-__global__ void __launch_bounds__(512) k_moments(MomArgs<T> a) {
+// Sum over the L lanes of an aligned lane group (every lane gets the same
+// bits: each butterfly level adds the same two operands in either order).
+template <int L> __device__ __forceinline__ double group_sum(double v) {
+#pragma unroll
+  for (int o = L / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Moment kernel: persistent warps; each warp takes R DG nodes (velocity rows)
+// at a time, L = 32/R lanes per row, from a per-warp ring of stages filled by
+// 1-D bulk copies, so f is read from HBM once for both passes and the R
+// rows' reductions and FP64 epilogues run side by side.
+template <class T, int R>
+__global__ void __launch_bounds__(512, 1) k_moments(MomArgs<T> a) {
   if (a.ctrl->done) return;
+  constexpr int L = 32 / R;
   extern __shared__ __align__(128) unsigned char sm_raw[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-  // layout: [barriers][tables 3*Vp][rings]
+  const int grp = lane / L, sub = lane % L;
+  // layout: [barriers][tables 3*Vp][rings: warp, stage, R rows]
   uint64_t* bars = reinterpret_cast<uint64_t*>(sm_raw) + warp * a.nstage;
   T* tb = reinterpret_cast<T*>(sm_raw + 128 * ((nwarp * a.nstage * 8 + 127) / 128));
+  const size_t stage_bytes = (size_t)R * a.rowbytes;
   unsigned char* ring =
-      reinterpret_cast<unsigned char*>(tb + 3 * (size_t)a.Vp) + (size_t)warp * a.nstage * a.rowbytes;
+      reinterpret_cast<unsigned char*>(tb + 3 * (size_t)a.Vp) + (size_t)warp * a.nstage * stage_bytes;
   for (int i = threadIdx.x; i < 3 * a.Vp; i += blockDim.x) tb[i] = a.tabs[i];
+  const int ngroups = (a.ndg + R - 1) / R;
   const int gw = blockIdx.x * nwarp + warp, stride = gridDim.x * nwarp;
   if (lane == 0) {
     for (int s = 0; s < a.nstage; ++s) mbar_init(&bars[s], 1);
     fence_mbar_init();
   }
   __syncthreads();
-  // prologue: fill the ring
+  // lane 0: the rows of group g into stage s
+  auto fill = [&](int s, int g) {
+    const int r0 = g * R, nr = min(R, a.ndg - r0);
+    mbar_expect_tx(&bars[s], (unsigned)nr * a.rowbytes);
+    for (int k = 0; k < nr; ++k)
+      bulk_load(ring + (size_t)s * stage_bytes + (size_t)k * a.rowbytes, a.f + (size_t)(r0 + k) * a.Vp,
+                a.rowbytes, &bars[s]);
+  };
   if (lane == 0)
-    for (int s = 0; s < a.nstage; ++s) {
-      const int node = gw + s * stride;
-      if (node < a.ndg) {
-        mbar_expect_tx(&bars[s], a.rowbytes);
-        bulk_load(ring + (size_t)s * a.rowbytes, a.f + (size_t)node * a.Vp, a.rowbytes, &bars[s]);
-      }
-    }
+    for (int s = 0; s < a.nstage; ++s)
+      if (gw + s * stride < ngroups) fill(s, gw + s * stride);
   const int nq = (int)(a.rowbytes / 16);
   uint32_t parity = 0;  // bit s: parity of stage s
   int s = 0;
   bool aborted = false;
-  for (int node = gw; node < a.ndg; node += stride) {
+  double mumax = 0.0;
+  for (int g = gw; g < ngroups; g += stride) {
     int ok = 1;
     if (lane == 0) ok = mbar_wait_bounded(&bars[s], (parity >> s) & 1) ? 1 : 0;
     ok = __shfl_sync(0xffffffffu, ok, 0);
@@ -250,12 +276,15 @@ __global__ void __launch_bounds__(512) k_moments(MomArgs<T> a) {
     }
     mbar_wait_bounded(&bars[s], (parity >> s) & 1);  // completed: returns at once
     parity ^= 1u << s;
-    const T* row = reinterpret_cast<const T*>(ring + (size_t)s * a.rowbytes);
+    const int node = g * R + grp;
+    const bool live = node < a.ndg;
+    const T* row = reinterpret_cast<const T*>(ring + (size_t)s * stage_bytes + (size_t)grp * a.rowbytes);
+    const int nql = live ? nq : 0;
     double s0 = 0, s1 = 0, s2 = 0;
-    RowMath<T>::pass1(row, tb, a.Vp, nq, lane, s0, s1, s2);
-    s0 = warp_sum(s0);
-    s1 = warp_sum(s1);
-    s2 = warp_sum(s2);
+    RowMath<T>::pass1(row, tb, a.Vp, nql, sub, L, s0, s1, s2);
+    s0 = group_sum<L>(s0);
+    s1 = group_sum<L>(s1);
+    s2 = group_sum<L>(s2);
     double nd = 0, ux = 0, uy = 0;
     if (s0 >= TINY_D) {  // src/macros.f90:126-134
       nd = s0;
@@ -263,20 +292,19 @@ __global__ void __launch_bounds__(512) k_moments(MomArgs<T> a) {
       uy = s2 / s0;
     }
     double sp = 0, sc = 0;
-    RowMath<T>::pass2(row, tb, a.Vp, nq, lane, ux, uy, sp, sc);
-    sp = warp_sum(sp);
-    sc = warp_sum(sc);
+    RowMath<T>::pass2(row, tb, a.Vp, nql, sub, L, ux, uy, sp, sc);
+    sp = group_sum<L>(sp);
+    sc = group_sum<L>(sc);
     __syncwarp();
-    // the row is consumed: refill this stage with the row nstage ahead
+    // the rows are consumed: refill this stage with the group nstage ahead
     if (lane == 0) {
-      const int nxt = node + a.nstage * stride;
-      if (nxt < a.ndg) {
+      const int nxt = g + a.nstage * stride;
+      if (nxt < ngroups) {
         fence_proxy_async_smem();
-        mbar_expect_tx(&bars[s], a.rowbytes);
-        bulk_load(ring + (size_t)s * a.rowbytes, a.f + (size_t)nxt * a.Vp, a.rowbytes, &bars[s]);
+        fill(s, nxt);
       }
     }
-    if (lane == 0) {
+    if (sub == 0 && live) {
       const double ps = sp * a.MM;
       const double ct = (nd >= TINY_D) ? sc / nd : 0.0;
       const double mu = sqrt(2.0) * ct * a.sigt * nd;
@@ -299,14 +327,21 @@ __global__ void __launch_bounds__(512) k_moments(MomArgs<T> a) {
       a.disuy[node] = uy;
       a.disps[node] = ps;
       a.mu[node] = mu;
-      atomicMax(reinterpret_cast<unsigned long long*>(&a.ctrl->maxmu), (unsigned long long)__double_as_longlong(mu));
+      mumax = fmax(mumax, mu);
     }
     s = (s + 1 == a.nstage) ? 0 : s + 1;
   }
-  if (aborted && lane == 0) {
-    a.ctrl->timeout = 1;
-    for (int k = 0; k < a.nstage; ++k) mbar_wait_bounded(&bars[k], (parity >> k) & 1);
+  if (aborted) {
+    if (lane == 0) {
+      a.ctrl->timeout = 1;
+      for (int k = 0; k < a.nstage; ++k) mbar_wait_bounded(&bars[k], (parity >> k) & 1);
+    }
+    return;
   }
+  // MU >= 0: the max of the bit patterns is the max of the values
+  mumax = warp_max(mumax);
+  if (lane == 0 && mumax > 0.0)
+    atomicMax(reinterpret_cast<unsigned long long*>(&a.ctrl->maxmu), (unsigned long long)__double_as_longlong(mumax));
 }
 
 // --------------------------------------------------------- wall flux ----
@@ -658,16 +693,20 @@ __global__ void __launch_bounds__(2 * EB, sizeof(T) == 4 ? 2 : 1)
     for (int k = 0; k < ntl; ++k) {
       const int bi = k & 1;
       unsigned char* const tl = base + (size_t)bi * tile_bytes;
-      const bool ok = mbar_wait_bounded(&bars[bi], (par >> bi) & 1u);
+      // thread 0 waits for the boxes (the others wait in the barrier, not
+      // spinning); every thread waits for its own halo copies
+      const uint32_t ph = (par >> bi) & 1u;
+      const bool ok = tid != 0 || mbar_wait_bounded(&bars[bi], ph);
       par ^= 1u << bi;
       cp_async_wait<0>();
-      // tile k has landed for every thread (or some wait expired), and every
-      // thread has written and fenced its new rows of tile k - 1
+      // tile k has landed (or the wait expired), and every thread has written
+      // and fenced its new rows of tile k - 1
       if (__syncthreads_or(ok ? 0 : 1)) {
         aborted = true;
         abort_buf = bi;
         break;
       }
+      if (tid != 0) mbar_try_wait(&bars[bi], ph);  // completed: acquires the box data
       if (tid == 0 && k > 0) store(vt0 + k - 1, bi ^ 1);
       const int vb0 = (vt0 + k) * VT;
       const T* vx = vtab + k * VT;

@@ -872,10 +872,13 @@ __global__ void __launch_bounds__(2 * EB, sizeof(T) == 4 ? 2 : 1)
                   rr = rr > (T)0 ? rr : (T)0;
                 }
                 T fn = f + d;
+                // L2 residual: the change the unknown receives (-f where
+                // the clip applies; none at inflow-reset nodes)
+                const T ch = (fn < (T)0) ? -f : d;
                 fn = fn > (T)0 ? fn : (T)0;
                 if (live) {
                   rmt = rr > rmt ? rr : rmt;
-                  sqt += d * d;
+                  if (!(flags & (1 << i))) sqt += ch * ch;
                 } else {
                   fn = (T)0;
                 }

@@ -24,8 +24,11 @@
 //
 // Extensions (each reduces to the reference when switched off):
 //   * moving walls: per-boundary-side wall velocity (zero -> reference Mw);
-//   * L2 residual: sqrt(sum DELUN^2) in double, next to the reference's
-//     max|DELUN| (RESIDUAL(IV), src/getinc.f90:22-43);
+//   * L2 residual: the L2 norm (in double) of the change the unknowns
+//     receive in a step -- DELUN, -f where ADTHEM clips, nothing at the DG
+//     nodes INFLOW resets (Dirichlet data) -- next to the reference's
+//     max|DELUN| (RESIDUAL(IV), src/getinc.f90:22-43), which keeps the
+//     increment INFLOW overwrites and so stalls on inflow meshes;
 //   * ring_fix: the physically intended speed ring in the wall-reflection
 //     lookup (off -> the reference formula of src/getbou.f90:223-244).
 #include <algorithm>
@@ -723,7 +726,9 @@ void getbou(Case<R>& c, Work<R>& w, int IEL, int IP1, int IN1, int IN2, R UX, R 
 // (src/getelc.f90:27-121), EDGFLXOPT (src/edgflxopt.f90:62-125, no partition
 // edges), RHS*DTE (src/advnce.f90:342-346), GETINC (src/getinc.f90:22-43) or
 // CMMINC (src/cmminc.f90:22-41), ADTHEM (src/adthem.f90:17-26) and INFLOW
-// (src/inflow.f90:23-59).  Returns RESIDUAL(IV); adds sum DELUN^2 to *l2.
+// (src/inflow.f90:23-59).  Returns RESIDUAL(IV); adds to *l2 the sum of
+// squares of the changes the unknowns receive (DELUN, -f where ADTHEM clips,
+// nothing at the DG nodes INFLOW resets).
 template <class R> R velocity_body(Case<R>& c, Work<R>& w, int IV, R DTE, double* l2) {
   const R PI = K<R>::PI(), NA = K<R>::NA(), C13 = K<R>::C13();
   const int E = c.NELEM, V = c.VNPNT;
@@ -849,7 +854,6 @@ template <class R> R velocity_body(Case<R>& c, Work<R>& w, int IV, R DTE, double
         R R1 = c.MMAT[i] * w.RHS[i] + COLL * DTE;
         if (std::fabs(R1) > std::fabs(RESIDUAL)) RESIDUAL = std::fabs(R1);
         w.DELUN[i] = w.DELUN[i] + c.MMAT[i] * w.RHS[i] + COLL * DTE;
-        sq += (double)w.DELUN[i] * (double)w.DELUN[i];
       }
   } else {
     for (int IE = 1; IE <= E; ++IE)
@@ -864,15 +868,17 @@ template <class R> R velocity_body(Case<R>& c, Work<R>& w, int IV, R DTE, double
           if (R1 > RESIDUAL) RESIDUAL = R1;
           w.DELUN[i] = w.DELUN[i] + CMM * w.RHS[i];
         }
-        sq += (double)w.DELUN[i] * (double)w.DELUN[i];
       }
   }
-  *l2 += sq;
-  // ADTHEM
+  // ADTHEM; the L2 residual (an extension) takes the change each unknown
+  // receives: DELUN, or -f where the positivity clip applies
   for (int IE = 1; IE <= E; ++IE)
     for (int IN = 1; IN <= 3; ++IN) {
       R& f = F(IN, IE);
-      f = f + w.DELUN[c2(IN, IE, 3)];
+      const size_t i = c2(IN, IE, 3);
+      const R fn = f + w.DELUN[i];
+      w.DELUN[i] = (fn < (R)0.0) ? -f : w.DELUN[i];
+      f = fn;
       if (f < (R)0.0) f = 0.0;
     }
   // INFLOW
@@ -891,10 +897,15 @@ template <class R> R velocity_body(Case<R>& c, Work<R>& w, int IV, R DTE, double
       for (int IE = 1; IE <= E; ++IE)
         for (int IN = 1; IN <= 3; ++IN) {
           int IPT = c.INTMA[c2(IN, IE, 3)];
-          if (IPT == IP1 || IPT == IP2) F(IN, IE) = nf;
+          if (IPT == IP1 || IPT == IP2) {
+            F(IN, IE) = nf;
+            w.DELUN[c2(IN, IE, 3)] = 0;  // Dirichlet data, not an unknown
+          }
         }
     }
   }
+  for (size_t i = 0; i < w.DELUN.size(); ++i) sq += (double)w.DELUN[i] * (double)w.DELUN[i];
+  *l2 += sq;
   return RESIDUAL;
 }
 
@@ -1122,7 +1133,7 @@ int orc_inicon2(void* vh, double T1, double P1, double U0, double V0) {
 }
 
 // Runs nsteps passes of the ADVNCE loop.  Per step: max|DELUN| (SUMRES), the
-// L2 norm of DELUN, and DTE.  Returns 0 or an error code.
+// L2 residual (see the header), and DTE.  Returns 0 or an error code.
 int orc_advance(void* vh, int nsteps, double* res_linf, double* res_l2, double* dte) {
   int err = 0;
   DISPATCH((Handle*)vh, {

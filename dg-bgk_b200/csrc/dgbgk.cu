@@ -91,16 +91,216 @@ struct ImplBase {
   float last_ms = 0.f;
 };
 
+// A set of cases launched together (one handle, or a batch): the case table
+// and the flattened work offsets on the device, and the launch shapes.
+template <class T> struct LaunchSet {
+  CaseDev<T>* d_cases = nullptr;
+  int* d_off = nullptr;  // [3][n + 1]: sweep units, moment row groups, wall sides
+  BatchCtl* d_ctl = nullptr;
+  BatchArgs<T> args{};
+  int n = 0, cap = 0, total_units = 0, total_groups = 0, total_walls = 0;
+  int eb = 128, immat = 1;
+  bool one = false;       // a single case: the kernels take it as a parameter
+  CaseDev<T> one_case{};  // that case (zeros for a batch)
+  int mom_rows = 1, mom_warps = 1, mom_grid = 1, sweep_grid = 1;
+  size_t mom_smem = 0, sweep_smem = 0;
+  ~LaunchSet() { release(); }
+  void release() {
+    dfree(d_cases);
+    dfree(d_off);
+    dfree(d_ctl);
+    cap = 0;
+  }
+};
+
+template <class T> using MomFn = void (*)(BatchArgs<T>, int, const CaseDev<T>);
+template <class T, bool ONE> MomFn<T> mom_fn1(int R) {
+  return R == 4 ? k_moments<T, 4, ONE> : R == 2 ? k_moments<T, 2, ONE> : k_moments<T, 1, ONE>;
+}
+template <class T> MomFn<T> mom_fn(int R, bool one) { return one ? mom_fn1<T, true>(R) : mom_fn1<T, false>(R); }
+template <class T> using SweepFn = void (*)(BatchArgs<T>, int, const CaseDev<T>);
+template <class T, bool ONE> SweepFn<T> sweep_fn1(int eb, int immat) {
+  if (eb == 64) return immat == 1 ? k_sweep<T, 64, 1, ONE> : k_sweep<T, 64, 0, ONE>;
+  return immat == 1 ? k_sweep<T, 128, 1, ONE> : k_sweep<T, 128, 0, ONE>;
+}
+template <class T> SweepFn<T> sweep_fn(int eb, int immat, bool one) {
+  return one ? sweep_fn1<T, true>(eb, immat) : sweep_fn1<T, false>(eb, immat);
+}
+
+// Lets a kernel take as much dynamic shared memory as the device allows.
+// The attribute is process-wide state of the function, shared by every
+// handle, so it is raised to the limit (each launch still asks for exactly
+// what it needs) rather than set to one handle's size.
+inline int allow_max_smem(const void* fn) {
+  int dev = 0, optin = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  cudaFuncAttributes fa;
+  CK(cudaFuncGetAttributes(&fa, fn));
+  CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes));
+  return 0;
+}
+
+// Resident sweep CTAs per SM for a tile shape (0: does not fit).
+template <class T> int sweep_per_sm(int eb, int immat, int max_halo, bool one) {
+  const size_t smem = SweepGeo<T>::smem(eb, max_halo);
+  if (smem > 227 * 1024) return 0;
+  SweepFn<T> fn = sweep_fn<T>(eb, immat, one);
+  if (allow_max_smem((const void*)fn) != 0) return 0;
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)fn, 2 * eb, smem) != cudaSuccess) return 0;
+  return per_sm;
+}
+
+// Velocity tiles per sweep work unit for a set of cases: about `upc` units
+// per resident CTA over the whole set, equal groups of tiles per case.
+inline int tiles_per_unit(long total_tiles, int grid0, int upc, int nvt) {
+  int t = (int)std::min<long>(16, std::max<long>(1, total_tiles / ((long)upc * grid0)));
+  const int ng = (nvt + t - 1) / t;
+  return (nvt + ng - 1) / ng;
+}
+
+// Uploads the case table and picks the launch shapes.  Moments: per-warp
+// rings of R-row stages; picks (R, warps per CTA, ring stages) with the most
+// resident warps per SM, then the most rows in flight, then the fewest rows
+// per warp step (measured on B200 at 24x48 velocities: one row per warp step
+// was fastest in FP32 and FP64).
+template <class T>
+int build_launch_set(LaunchSet<T>& L, const std::vector<CaseDev<T>>& cs, int eb, int immat, int max_halo, int nsm,
+                     cudaStream_t st, int force_rows = 0) {
+  const int n = (int)cs.size();
+  const bool one = n == 1;
+  unsigned maxrow = 16;
+  for (const auto& c : cs) maxrow = std::max(maxrow, c.rowbytes);
+  // one case: its moment tables sit in shared memory
+  const size_t tbytes = one ? (3 * (size_t)cs[0].Vp * sizeof(T) + 127) / 128 * 128 : 0;
+  const size_t cap = 227 * 1024, sm_total = 228 * 1024;
+  long best = -1;
+  for (int R : {4, 2, 1})
+    for (int w : {16, 12, 10, 8, 6, 5, 4, 3, 2, 1})
+      for (int sg : {3, 2}) {
+        if (force_rows > 0 && R != force_rows) continue;
+        const size_t bytes = 128 * (((size_t)w * sg * 8 + 127) / 128) + tbytes + (size_t)w * sg * R * maxrow;
+        if (bytes > cap) continue;
+        const int blocks = (int)std::min<size_t>(4, sm_total / (bytes + 1024));
+        if (blocks < 1) continue;
+        const long score = ((long)blocks * w * 1024 + (long)blocks * w * (sg - 1) * R) * 8 + (8 - R);
+        if (score > best) {
+          best = score;
+          L.mom_rows = R;
+          L.mom_warps = w;
+          L.args.mom_stages = sg;
+          L.mom_smem = bytes;
+        }
+      }
+  if (best < 0) {
+    set_error("velocity rows too long for the moment kernel's shared-memory ring");
+    return DGBGK_EUNSUP;
+  }
+  std::vector<int> off(3 * (size_t)(n + 1), 0);
+  for (int c = 0; c < n; ++c) {
+    const auto& k = cs[c];
+    const int units = k.nblocks * ((k.nvt + k.tpu - 1) / k.tpu);
+    const int groups = (3 * k.E + L.mom_rows - 1) / L.mom_rows;
+    off[c + 1] = off[c] + units;
+    off[(n + 1) + c + 1] = off[(n + 1) + c] + groups;
+    off[2 * (n + 1) + c + 1] = off[2 * (n + 1) + c] + k.nwall;
+  }
+  if (n > L.cap) {
+    L.release();
+    TRY(dalloc(&L.d_cases, n));
+    TRY(dalloc(&L.d_off, 3 * (size_t)(n + 1)));
+    TRY(dalloc(&L.d_ctl, 1));
+    L.cap = n;
+  }
+  CK(cudaMemcpyAsync(L.d_cases, cs.data(), n * sizeof(CaseDev<T>), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(L.d_off, off.data(), off.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+  CK(cudaMemsetAsync(L.d_ctl, 0, sizeof(BatchCtl), st));
+  L.n = n;
+  L.one = one;
+  L.one_case = one ? cs[0] : CaseDev<T>{};
+  L.eb = eb;
+  L.immat = immat;
+  L.total_units = off[n];
+  L.total_groups = off[(n + 1) + n];
+  L.total_walls = off[2 * (n + 1) + n];
+  L.args.cases = L.d_cases;
+  L.args.unit_off = L.d_off;
+  L.args.grp_off = L.d_off + (n + 1);
+  L.args.wall_off = L.d_off + 2 * (n + 1);
+  L.args.ctl = L.d_ctl;
+  L.args.ncases = n;
+  L.args.max_halo = max_halo;
+  L.args.mom_rowbytes = maxrow;
+  // moments: persistent grid
+  MomFn<T> mf = mom_fn<T>(L.mom_rows, one);
+  TRY(allow_max_smem((const void*)mf));
+  int per_sm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)mf, L.mom_warps * 32, L.mom_smem));
+  per_sm = std::max(per_sm, 1);
+  L.mom_grid = std::max(1, std::min((L.total_groups + L.mom_warps - 1) / L.mom_warps, per_sm * nsm));
+  // sweep: persistent grid
+  const int sps = sweep_per_sm<T>(eb, immat, max_halo, one);
+  if (sps < 1) {
+    set_error("sweep kernel does not fit on an SM with this tile");
+    return DGBGK_EUNSUP;
+  }
+  L.sweep_smem = SweepGeo<T>::smem(eb, max_halo);
+  L.sweep_grid = std::max(1, std::min(L.total_units, sps * nsm));
+  return 0;
+}
+
+// Reports a failed launch with its kernel and configuration.
+inline int launch_check(const char* what, int grid, int block, size_t smem) {
+  const cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) return 0;
+  set_error(std::string("CUDA error: ") + cudaGetErrorString(e) + " (launch of " + what + ": grid " +
+            std::to_string(grid) + ", block " + std::to_string(block) + ", dynamic smem " + std::to_string(smem) +
+            ")");
+  return DGBGK_ECUDA;
+}
+
+// One pseudo-time step of every case of the set: moments, wall flux, sweep,
+// residual bookkeeping.
+template <class T> int enqueue_step(const LaunchSet<T>& L, cudaStream_t st, float* ms = nullptr) {
+  cudaEvent_t ev[5];
+  if (ms)
+    for (auto& e : ev) CK(cudaEventCreate(&e));
+  if (ms) cudaEventRecord(ev[0], st);
+  mom_fn<T>(L.mom_rows, L.one)<<<L.mom_grid, L.mom_warps * 32, L.mom_smem, st>>>(L.args, L.total_groups,
+                                                                                 L.one_case);
+  TRY(launch_check("k_moments", L.mom_grid, L.mom_warps * 32, L.mom_smem));
+  if (ms) cudaEventRecord(ev[1], st);
+  if (L.total_walls > 0) {
+    k_wall<T><<<(L.total_walls + 7) / 8, 256, 0, st>>>(L.args, L.total_walls);
+    TRY(launch_check("k_wall", (L.total_walls + 7) / 8, 256, 0));
+  }
+  if (ms) cudaEventRecord(ev[2], st);
+  sweep_fn<T>(L.eb, L.immat, L.one)<<<L.sweep_grid, 2 * L.eb, L.sweep_smem, st>>>(L.args, L.total_units,
+                                                                                   L.one_case);
+  TRY(launch_check("k_sweep", L.sweep_grid, 2 * L.eb, L.sweep_smem));
+  if (ms) cudaEventRecord(ev[3], st);
+  k_resid<T><<<L.n, 32, 0, st>>>(L.args);
+  TRY(launch_check("k_resid", L.n, 32, 0));
+  if (ms) {
+    cudaEventRecord(ev[4], st);
+    cudaEventSynchronize(ev[4]);
+    for (int k = 0; k < 4; ++k) cudaEventElapsedTime(&ms[k], ev[k], ev[k + 1]);
+    for (auto& e : ev) cudaEventDestroy(e);
+  }
+  return 0;
+}
+
 template <class T> struct Impl : ImplBase {
+  static constexpr int GRAPH_STEPS = 2;  // pseudo-time steps per graph launch
   cudaStream_t st = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, evpoll[2] = {nullptr, nullptr};
-  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
-  int cur = 0;
+  cudaGraphExec_t gexec = nullptr;
+  int cur = 0;  // host copy of Ctrl::cur
   int tpu = 1;  // velocity tiles per sweep work unit
   int Vp = 0;
   // device arrays
   T* f[2] = {nullptr, nullptr};
-  CUtensorMap tm[2];  // f[b] as a 2-D tensor of rows (sweep tile boxes)
   ElemRec<T>* rec = nullptr;
   int *halo_off = nullptr, *halo_list = nullptr;
   T *cmax = nullptr, *cmin = nullptr;
@@ -113,10 +313,6 @@ template <class T> struct Impl : ImplBase {
   WallSide* walls = nullptr;
   int *node_off = nullptr, *node_dg = nullptr;
   double* node_ae = nullptr;
-  double *part_max = nullptr, *part_sq = nullptr;
-  int nparts = 0, sweep_grid = 0, part_cap = 0;
-  int mom_grid = 0, mom_warps = 0, mom_stages = 0, mom_rows = 4;
-  size_t mom_smem = 0;
   double *hist_linf = nullptr, *hist_l2 = nullptr, *hist_dt = nullptr;
   int hist_cap = 0;
   Ctrl* ctrl = nullptr;
@@ -124,11 +320,14 @@ template <class T> struct Impl : ImplBase {
   void* staging = nullptr;
   size_t staging_bytes = 0;
   int* d_inv = nullptr;
+  CaseDev<T> hc;          // this case's table entry
+  LaunchSet<T> single;    // this case alone
 
   ~Impl() override {
     cudaSetDevice(device);
     if (st) cudaStreamSynchronize(st);
     drop_graphs();
+    single.release();
     dfree(d_inv);
     dfree(f[0]);
     dfree(f[1]);
@@ -157,8 +356,6 @@ template <class T> struct Impl : ImplBase {
     dfree(node_off);
     dfree(node_dg);
     dfree(node_ae);
-    dfree(part_max);
-    dfree(part_sq);
     dfree(hist_linf);
     dfree(hist_l2);
     dfree(hist_dt);
@@ -174,7 +371,6 @@ template <class T> struct Impl : ImplBase {
 
   int nvt() const { return (pl.V + SweepGeo<T>::VT - 1) / SweepGeo<T>::VT; }
   static int default_eb() { return 128; }
-  size_t sweep_smem() const { return SweepGeo<T>::smem(pl.EB, pl.max_halo); }
 
   int init(int tile_elems) {
     CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
@@ -232,59 +428,11 @@ template <class T> struct Impl : ImplBase {
     CK(cudaMallocHost((void**)&hctrl, 3 * sizeof(Ctrl)));
     std::memset(hctrl, 0, 3 * sizeof(Ctrl));
     CK(cudaMemcpyAsync(ctrl, hctrl, sizeof(Ctrl), cudaMemcpyHostToDevice, st));
-    TRY(config_moments());
-    TRY(set_tile(tile_elems));
     TRY(ensure_hist(1024));
+    TRY(set_tile(tile_elems, 8));
     CK(cudaStreamSynchronize(st));
     return 0;
   }
-
-  // Moment kernel: per-warp rings of velocity rows, persistent grid.  Picks
-  // the (warps per CTA, ring stages) with the most resident warps per SM.
-  // Moment kernel: per-warp rings of R-row stages, persistent grid.  Picks
-  // (rows per warp step R, warps per CTA, ring stages) with the most resident
-  // warps per SM, then the most rows in flight, then the fewest rows per warp
-  // step (measured on B200 at 24x48 velocities: one row per warp step was
-  // fastest in FP32 and FP64).
-  int config_moments() {
-    const size_t rowbytes = ((size_t)pl.V * sizeof(T) + 15) / 16 * 16;
-    const size_t tbytes = 3 * (size_t)Vp * sizeof(T);
-    const size_t cap = 227 * 1024, sm_total = 228 * 1024;
-    long best = -1;
-    for (int R : {4, 2, 1})
-      for (int w : {16, 12, 10, 8, 6, 5, 4, 3, 2, 1})
-        for (int sg : {3, 2}) {
-          const size_t bytes =
-              128 * (((size_t)w * sg * 8 + 127) / 128) + tbytes + (size_t)w * sg * R * rowbytes;
-          if (bytes > cap) continue;
-          const int blocks = (int)std::min<size_t>(4, sm_total / (bytes + 1024));
-          if (blocks < 1) continue;
-          const long score = ((long)blocks * w * 1024 + (long)blocks * w * (sg - 1) * R) * 8 + (8 - R);
-          if (score > best) {
-            best = score;
-            mom_rows = R;
-            mom_warps = w;
-            mom_stages = sg;
-            mom_smem = bytes;
-          }
-        }
-    if (best < 0) {
-      set_error("velocity rows too long for the moment kernel's shared-memory ring");
-      return DGBGK_EUNSUP;
-    }
-    const int warps = mom_warps;
-    MomFn fn = mom_fn();
-    CK(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mom_smem));
-    int per_sm = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)fn, warps * 32, mom_smem));
-    if (per_sm < 1) per_sm = 1;
-    const int ngroups = (3 * pl.E + mom_rows - 1) / mom_rows;
-    const int need = (ngroups + warps - 1) / warps;
-    mom_grid = std::max(1, std::min(need, per_sm * nsm));
-    return 0;
-  }
-  using MomFn = void (*)(MomArgs<T>);
-  MomFn mom_fn() const { return mom_rows == 4 ? k_moments<T, 4> : mom_rows == 2 ? k_moments<T, 2> : k_moments<T, 1>; }
 
   // f[b] as a [3E rows][Vp] tensor; box = one 64-byte velocity segment of
   // BOX_ROWS rows, 64-byte swizzle (the sweep's tile layout)
@@ -300,7 +448,7 @@ template <class T> struct Impl : ImplBase {
     cuuint32_t box[2] = {(cuuint32_t)SweepGeo<T>::VT, (cuuint32_t)SweepGeo<T>::BOX_ROWS};
     cuuint32_t estr[2] = {1, 1};
     for (int b = 0; b < 2; ++b) {
-      CUresult r = enc(&tm[b], dt, 2, f[b], dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+      CUresult r = enc(&hc.tm[b], dt, 2, f[b], dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                        CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
       if (r != CUDA_SUCCESS) {
         set_error("cuTensorMapEncodeTiled failed for the state buffer");
@@ -310,15 +458,61 @@ template <class T> struct Impl : ImplBase {
     return 0;
   }
 
-  using SweepFn = void (*)(const CUtensorMap, const CUtensorMap, SweepArgs<T>);
-  SweepFn sweep_fn() const {
-    if (pl.EB == 64) return pl.immat == 1 ? k_sweep<T, 64, 1> : k_sweep<T, 64, 0>;
-    return pl.immat == 1 ? k_sweep<T, 128, 1> : k_sweep<T, 128, 0>;
+  // this case's table entry (the tensor maps are set by make_tensor_maps)
+  void fill_case() {
+    hc.f[0] = f[0];
+    hc.f[1] = f[1];
+    hc.rec = rec;
+    hc.halo_off = halo_off;
+    hc.halo_list = halo_list;
+    hc.cx = cxT;
+    hc.cy = cyT;
+    hc.nfinf = nfT;
+    hc.tabs = tabs;
+    hc.bTw = bTw;
+    hc.bUw = bUw;
+    hc.bEta = bEta;
+    hc.bEtaD = bEtaD;
+    hc.cxD = cxD;
+    hc.cyD = cyD;
+    hc.wjf = wjf;
+    hc.walls = walls;
+    hc.cmax = cmax;
+    hc.cmin = cmin;
+    hc.nraw = nraw;
+    hc.disux = disux;
+    hc.disuy = disuy;
+    hc.disps = disps;
+    hc.mu = mu;
+    hc.hist_linf = hist_linf;
+    hc.hist_l2 = hist_l2;
+    hc.hist_dt = hist_dt;
+    hc.ctrl = ctrl;
+    hc.MM = pl.M / 6.022e26;
+    hc.sigt = 3.1416 * pl.d * pl.d;
+    hc.alpha = (T)pl.alpha;
+    hc.rgas = (T)pl.rgas;
+    hc.E = pl.E;
+    hc.V = pl.V;
+    hc.Vp = Vp;
+    hc.nblocks = pl.nblocks;
+    hc.nvt = nvt();
+    hc.tpu = tpu;
+    hc.nwall = (int)pl.walls.size();
+    hc.rowbytes = (unsigned)(((size_t)pl.V * sizeof(T) + 15) / 16 * 16);
+  }
+
+  // the one-case launch set
+  int refresh() {
+    fill_case();
+    TRY(build_launch_set(single, std::vector<CaseDev<T>>{hc}, pl.EB, pl.immat, pl.max_halo, nsm, st));
+    drop_graphs();
+    return 0;
   }
 
   // Sweep tile: EB elements per CTA (2*EB threads) x one 64-byte velocity
-  // segment.
-  int set_tile(int tile_elems) {
+  // segment; `upc` work units per resident CTA picks the tiles per unit.
+  int set_tile(int tile_elems, int upc) {
     const int eb = tile_elems > 0 ? tile_elems : default_eb();
     if (eb != 64 && eb != 128) {
       set_error("tile_elems must be 64 or 128");
@@ -356,38 +550,18 @@ template <class T> struct Impl : ImplBase {
       }
       TRY(upload(&rec, r, st));
     }
-    if (sweep_smem() > 227 * 1024) {
+    if (SweepGeo<T>::smem(pl.EB, pl.max_halo) > 227 * 1024) {
       set_error("sweep tile needs more than 227 KB of shared memory");
       return DGBGK_EUNSUP;
     }
     TRY(make_tensor_maps());
-    SweepFn fn = sweep_fn();
-    CK(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sweep_smem()));
-    int per_sm = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)fn, 2 * pl.EB, sweep_smem()));
-    if (per_sm < 1) {
+    const int sps = sweep_per_sm<T>(pl.EB, pl.immat, pl.max_halo, true);
+    if (sps < 1) {
       set_error("sweep kernel does not fit on an SM with this tile");
       return DGBGK_EUNSUP;
     }
-    // velocity tiles per work unit: about eight units per resident CTA, so
-    // the dynamic hand-out balances, and equal groups of tiles
-    const int grid0 = per_sm * nsm;
-    const long total = (long)pl.nblocks * nvt();
-    tpu = (int)std::min<long>(SweepGeo<T>::TPU_MAX, std::max<long>(1, total / (8L * grid0)));
-    const int ngroups = (nvt() + tpu - 1) / tpu;
-    tpu = (nvt() + ngroups - 1) / ngroups;
-    const int nunits = pl.nblocks * ngroups;
-    sweep_grid = std::max(1, std::min(nunits, grid0));
-    if (sweep_grid > part_cap) {
-      dfree(part_max);
-      dfree(part_sq);
-      TRY(dalloc(&part_max, sweep_grid));
-      TRY(dalloc(&part_sq, sweep_grid));
-      part_cap = sweep_grid;
-    }
-    nparts = sweep_grid;
-    drop_graphs();
-    return 0;
+    tpu = tiles_per_unit((long)pl.nblocks * nvt(), sps * nsm, upc, nvt());
+    return refresh();
   }
 
   int ensure_hist(int n) {
@@ -399,117 +573,43 @@ template <class T> struct Impl : ImplBase {
     TRY(dalloc(&hist_l2, n));
     TRY(dalloc(&hist_dt, n));
     hist_cap = n;
-    drop_graphs();
-    return 0;
-  }
-
-  // -------------------------------------------------------- launches ----
-  int launch_moments(int src) {
-    MomArgs<T> a;
-    a.f = f[src];
-    a.tabs = tabs;
-    a.rec = rec;
-    a.nraw = nraw;
-    a.disux = disux;
-    a.disuy = disuy;
-    a.disps = disps;
-    a.mu = mu;
-    a.ctrl = ctrl;
-    a.ndg = 3 * pl.E;
-    a.V = pl.V;
-    a.Vp = Vp;
-    a.nstage = mom_stages;
-    a.rowbytes = (unsigned)(((size_t)pl.V * sizeof(T) + 15) / 16 * 16);
-    a.MM = pl.M / 6.022e26;
-    a.sigt = 3.1416 * pl.d * pl.d;
-    CK(cudaMemsetAsync(&ctrl->maxmu, 0, sizeof(double), st));
-    mom_fn()<<<mom_grid, mom_warps * 32, mom_smem, st>>>(a);
-    CK(cudaGetLastError());
-    return 0;
-  }
-  int launch_wall(int src) {
-    if (pl.walls.empty()) return 0;
-    WallArgs<T> a{f[src], walls, cxD, cyD, wjf, bEta, bEtaD, ctrl, (int)pl.walls.size(), pl.V, Vp};
-    k_wall<T><<<(a.nwall + 7) / 8, 256, 0, st>>>(a);
-    CK(cudaGetLastError());
-    return 0;
-  }
-  int launch_sweep(int src) {
-    SweepArgs<T> a;
-    a.fin = f[src];
-    a.fout = f[1 - src];
-    a.rec = rec;
-    a.halo_off = halo_off;
-    a.halo_list = halo_list;
-    a.cx = cxT;
-    a.cy = cyT;
-    a.nfinf = nfT;
-    a.bTw = bTw;
-    a.bUw = bUw;
-    a.bEta = bEta;
-    a.cmax = cmax;
-    a.cmin = cmin;
-    a.part_max = part_max;
-    a.part_sq = part_sq;
-    a.ctrl = ctrl;
-    a.E = pl.E;
-    a.V = pl.V;
-    a.Vp = Vp;
-    a.nblocks = pl.nblocks;
-    a.max_halo = pl.max_halo;
-    a.nvt = nvt();
-    a.tpu = tpu;
-    a.alpha = (T)pl.alpha;
-    a.rgas = (T)pl.rgas;
-    sweep_fn()<<<sweep_grid, 2 * pl.EB, sweep_smem(), st>>>(tm[src], tm[1 - src], a);
-    CK(cudaGetLastError());
-    return 0;
-  }
-  int launch_resid() {
-    ResidArgs a{part_max, part_sq, hist_linf, hist_l2, hist_dt, ctrl};
-    k_resid<<<1, 1024, 0, st>>>(a);
-    CK(cudaGetLastError());
-    return 0;
-  }
-  int enqueue_step(int src) {
-    TRY(launch_moments(src));
-    TRY(launch_wall(src));
-    TRY(launch_sweep(src));
-    TRY(launch_resid());
+    if (halo_off) TRY(refresh());
     return 0;
   }
 
   void drop_graphs() {
-    for (auto& g : gexec)
-      if (g) {
-        cudaGraphExecDestroy(g);
-        g = nullptr;
-      }
+    if (gexec) {
+      cudaGraphExecDestroy(gexec);
+      gexec = nullptr;
+    }
   }
-  // Two pseudo-time steps (f[s] -> f[1-s] -> f[s]) as one graph.
-  int build_graph(int s) {
-    if (gexec[s]) return 0;
+  // GRAPH_STEPS pseudo-time steps as one graph (the buffer swap is on the
+  // device, so one graph serves every step)
+  int build_graph() {
+    if (gexec) return 0;
     cudaGraph_t g;
     CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-    int rc = enqueue_step(s);
-    if (rc == 0) rc = enqueue_step(1 - s);
+    int rc = 0;
+    for (int k = 0; k < GRAPH_STEPS && rc == 0; ++k) rc = enqueue_step(single, st);
     cudaError_t e = cudaStreamEndCapture(st, &g);
     if (rc != 0) return rc;
     CK(e);
-    CK(cudaGraphInstantiate(&gexec[s], g, 0));
+    CK(cudaGraphInstantiate(&gexec, g, 0));
     cudaGraphDestroy(g);
     return 0;
   }
 
-  int upload_ctrl(int max_steps, double tol) {
-    Ctrl& h = hctrl[0];
+  void fill_ctrl(Ctrl& h, int max_steps, double tol) const {
     std::memset(&h, 0, sizeof(Ctrl));
     h.max_steps = max_steps;
     h.tol = tol;
     h.ref = ref_host;
     h.dtc = pl.dtc;
-    h.nparts = nparts;
-    CK(cudaMemcpyAsync(ctrl, &h, sizeof(Ctrl), cudaMemcpyHostToDevice, st));
+    h.cur = cur;
+  }
+  int upload_ctrl(int max_steps, double tol) {
+    fill_ctrl(hctrl[0], max_steps, tol);
+    CK(cudaMemcpyAsync(ctrl, &hctrl[0], sizeof(Ctrl), cudaMemcpyHostToDevice, st));
     return 0;
   }
 
@@ -525,6 +625,20 @@ template <class T> struct Impl : ImplBase {
     return 0;
   }
 
+  // after an advance: step count, history, reference and current buffer
+  int collect(const Ctrl& c, int* steps, double* linf, double* l2, double* dt) {
+    const int ns = c.step;
+    if (steps) *steps = ns;
+    ref_host = c.ref;
+    cur = c.cur;
+    if (ns > 0) {
+      if (linf) CK(cudaMemcpy(linf, hist_linf, ns * sizeof(double), cudaMemcpyDeviceToHost));
+      if (l2) CK(cudaMemcpy(l2, hist_l2, ns * sizeof(double), cudaMemcpyDeviceToHost));
+      if (dt) CK(cudaMemcpy(dt, hist_dt, ns * sizeof(double), cudaMemcpyDeviceToHost));
+    }
+    return finish_status(c);
+  }
+
   int advance(int max_steps, double tol, int* steps, double* linf, double* l2, double* dt) override {
     if (max_steps < 0) {
       set_error("max_steps < 0");
@@ -534,17 +648,16 @@ template <class T> struct Impl : ImplBase {
     if (max_steps == 0) return 0;
     CK(cudaSetDevice(device));
     TRY(ensure_hist(max_steps));
-    const int s0 = cur;
-    TRY(build_graph(s0));
+    TRY(build_graph());
     TRY(upload_ctrl(max_steps, tol));
     CK(cudaEventRecord(ev0, st));
-    const int launches = (max_steps + 1) / 2;
+    const int launches = (max_steps + GRAPH_STEPS - 1) / GRAPH_STEPS;
     const int chunk = 32;
     int issued = 0, chunks = 0;
     bool stop = false;
     while (issued < launches && !stop) {
       const int n = std::min(chunk, launches - issued);
-      for (int i = 0; i < n; ++i) CK(cudaGraphLaunch(gexec[s0], st));
+      for (int i = 0; i < n; ++i) CK(cudaGraphLaunch(gexec, st));
       issued += n;
       const int slot = 1 + (chunks & 1);
       CK(cudaMemcpyAsync(&hctrl[slot], ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));
@@ -560,51 +673,22 @@ template <class T> struct Impl : ImplBase {
     CK(cudaMemcpyAsync(&hctrl[1], ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     CK(cudaEventElapsedTime(&last_ms, ev0, ev1));
-    const Ctrl c = hctrl[1];
-    const int ns = c.step;
-    if (steps) *steps = ns;
-    ref_host = c.ref;
-    if (ns > 0) {
-      if (linf) CK(cudaMemcpy(linf, hist_linf, ns * sizeof(double), cudaMemcpyDeviceToHost));
-      if (l2) CK(cudaMemcpy(l2, hist_l2, ns * sizeof(double), cudaMemcpyDeviceToHost));
-      if (dt) CK(cudaMemcpy(dt, hist_dt, ns * sizeof(double), cudaMemcpyDeviceToHost));
-    }
-    cur = s0 ^ (ns & 1);
-    return finish_status(c);
+    return collect(hctrl[1], steps, linf, l2, dt);
   }
 
   int profile(int nsteps, double* ms) override {
     CK(cudaSetDevice(device));
     TRY(ensure_hist(std::max(nsteps, 1)));
     TRY(upload_ctrl(nsteps, 0.0));
-    cudaEvent_t ev[5];
-    for (auto& e : ev) CK(cudaEventCreate(&e));
     double acc[4] = {0, 0, 0, 0};
-    int rc = 0;
-    for (int s = 0; s < nsteps && rc == 0; ++s) {
-      cudaEventRecord(ev[0], st);
-      rc = launch_moments(cur);
-      cudaEventRecord(ev[1], st);
-      if (rc == 0) rc = launch_wall(cur);
-      cudaEventRecord(ev[2], st);
-      if (rc == 0) rc = launch_sweep(cur);
-      cudaEventRecord(ev[3], st);
-      if (rc == 0) rc = launch_resid();
-      cudaEventRecord(ev[4], st);
-      cudaEventSynchronize(ev[4]);
-      for (int k = 0; k < 4; ++k) {
-        float t = 0;
-        cudaEventElapsedTime(&t, ev[k], ev[k + 1]);
-        acc[k] += t;
-      }
-      cur ^= 1;
+    for (int s = 0; s < nsteps; ++s) {
+      float k[4] = {0, 0, 0, 0};
+      TRY(enqueue_step(single, st, k));
+      for (int i = 0; i < 4; ++i) acc[i] += k[i];
     }
-    for (auto& e : ev) cudaEventDestroy(e);
-    if (rc) return rc;
     CK(cudaMemcpy(&hctrl[1], ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost));
-    ref_host = hctrl[1].ref;
     for (int k = 0; k < 4; ++k) ms[k] = nsteps > 0 ? acc[k] / nsteps : 0.0;
-    return finish_status(hctrl[1]);
+    return collect(hctrl[1], nullptr, nullptr, nullptr, nullptr);
   }
 
   // auxiliary kernels run with done = 0
@@ -722,7 +806,9 @@ template <class T> struct Impl : ImplBase {
 
   int moments_now() {
     TRY(aux_ctrl());
-    TRY(launch_moments(cur));
+    mom_fn<T>(single.mom_rows, true)<<<single.mom_grid, single.mom_warps * 32, single.mom_smem, st>>>(
+        single.args, single.total_groups, single.one_case);
+    CK(cudaGetLastError());
     return 0;
   }
 
@@ -801,7 +887,10 @@ template <class T> struct Impl : ImplBase {
     CK(cudaSetDevice(device));
     TRY(aux_ctrl());
     CK(cudaMemsetAsync(bEtaD, 0, std::max(pl.B, 1) * sizeof(double), st));
-    TRY(launch_wall(cur));
+    if (single.total_walls > 0) {
+      k_wall<T><<<(single.total_walls + 7) / 8, 256, 0, st>>>(single.args, single.total_walls);
+      CK(cudaGetLastError());
+    }
     if (pl.B) CK(cudaMemcpyAsync(eta, bEtaD, pl.B * sizeof(double), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     return 0;
@@ -973,6 +1062,371 @@ int dgbgk_profile_steps(dgbgk_handle* h, int nsteps, double* kernel_ms) {
   return h->impl->profile(nsteps, kernel_ms);
 }
 void dgbgk_destroy(dgbgk_handle* h) { delete h; }
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Batches: many handles advanced by one launch set (one persistent launch
+// per kernel and step, captured in a CUDA graph).
+namespace {
+
+// 1 when every case of the set is done
+template <class T> __global__ void k_all_done(BatchArgs<T> a, int* out) {
+  int active = 0;
+  for (int c = threadIdx.x; c < a.ncases; c += blockDim.x) active |= !a.cases[c].ctrl->done;
+  active = __syncthreads_or(active);
+  if (threadIdx.x == 0) *out = !active;
+}
+
+struct BatchBase {
+  virtual ~BatchBase() {}
+  virtual int advance(int max_steps, double tol, int* steps, double* l2) = 0;
+  virtual void info(int* out) const = 0;
+  virtual int tuning(int n, double* ms) const = 0;
+  float last_ms = 0.f;
+};
+
+template <class T> struct BatchImpl : BatchBase {
+  static constexpr int GRAPH_STEPS = 2;
+  std::vector<Impl<T>*> cs;
+  LaunchSet<T> L;
+  int device = 0, nsm = 148, eb = 128, upc = 8, immat = 1, max_halo = 0;
+  cudaStream_t st = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, evp[2] = {nullptr, nullptr};
+  cudaGraphExec_t gexec = nullptr;
+  int* d_done = nullptr;
+  int* h_done = nullptr;  // pinned [2]
+  int rows = 0;           // moment rows per warp step (0: the heuristic)
+  // ms per step: (eb 64, 128) x (upc 2, 4, 8, 16), then moment rows 1, 2, 4;
+  // 0 = not tried
+  std::vector<double> tune_ms;
+
+  ~BatchImpl() override {
+    cudaSetDevice(device);
+    if (st) cudaStreamSynchronize(st);
+    if (gexec) cudaGraphExecDestroy(gexec);
+    L.release();
+    dfree(d_done);
+    if (h_done) cudaFreeHost(h_done);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    for (auto& e : evp)
+      if (e) cudaEventDestroy(e);
+    if (st) cudaStreamDestroy(st);
+  }
+
+  int init(std::vector<Impl<T>*> cases) {
+    cs = std::move(cases);
+    device = cs[0]->device;
+    nsm = cs[0]->nsm;
+    immat = cs[0]->pl.immat;
+    for (auto* c : cs) {
+      if (c->device != device || c->pl.immat != immat) {
+        set_error("dgbgk_batch_create: cases must share the device, the precision and IMMAT");
+        return DGBGK_EINVAL;
+      }
+    }
+    CK(cudaSetDevice(device));
+    CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    CK(cudaEventCreate(&ev0));
+    CK(cudaEventCreate(&ev1));
+    for (auto& e : evp) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    TRY(dalloc(&d_done, 1));
+    CK(cudaMallocHost((void**)&h_done, 2 * sizeof(int)));
+    tune_ms.assign(11, 0.0);
+    return 0;
+  }
+
+  // Re-blocks every case to EB = e and gives each case its tiles per unit
+  // from the whole batch's work (about u units per resident CTA).
+  int configure(int e, int u) {
+    for (auto* c : cs) {
+      TRY(c->set_tile(e, u));
+      CK(cudaStreamSynchronize(c->st));
+    }
+    max_halo = 0;
+    long tiles = 0;
+    for (auto* c : cs) {
+      max_halo = std::max(max_halo, c->pl.max_halo);
+      tiles += (long)c->pl.nblocks * c->nvt();
+    }
+    const int sps = sweep_per_sm<T>(e, immat, max_halo, cs.size() == 1);
+    if (sps < 1) {
+      set_error("dgbgk_batch: the sweep tile does not fit on an SM");
+      return DGBGK_EUNSUP;
+    }
+    std::vector<CaseDev<T>> table;
+    for (auto* c : cs) {
+      c->hc.tpu = tiles_per_unit(tiles, sps * nsm, u, c->nvt());
+      table.push_back(c->hc);
+    }
+    TRY(build_launch_set(L, table, e, immat, max_halo, nsm, st, rows));
+    eb = e;
+    upc = u;
+    if (gexec) {
+      cudaGraphExecDestroy(gexec);
+      gexec = nullptr;
+    }
+    return 0;
+  }
+
+  int upload_ctrls(int max_steps, double tol) {
+    for (auto* c : cs) {
+      c->fill_ctrl(c->hctrl[0], max_steps, tol);
+      CK(cudaMemcpyAsync(c->ctrl, &c->hctrl[0], sizeof(Ctrl), cudaMemcpyHostToDevice, st));
+    }
+    return 0;
+  }
+
+  // Autotuner: times `steps` steps (after one untimed) of every candidate
+  // tile shape on the cases' current states, restoring the states after
+  // each, and keeps the fastest.
+  int autotune(int fixed_eb, int fixed_upc, int steps) {
+    std::vector<T*> backup(cs.size(), nullptr);
+    int rc = 0;
+    for (size_t i = 0; i < cs.size() && rc == 0; ++i) {
+      const size_t n = (size_t)3 * cs[i]->pl.E * cs[i]->Vp;
+      rc = dalloc(&backup[i], n);
+      if (rc == 0 && cudaMemcpyAsync(backup[i], cs[i]->f[cs[i]->cur], n * sizeof(T), cudaMemcpyDeviceToDevice, st) !=
+                         cudaSuccess)
+        rc = DGBGK_ECUDA;
+    }
+    auto restore = [&]() -> int {
+      for (size_t i = 0; i < cs.size(); ++i) {
+        const size_t n = (size_t)3 * cs[i]->pl.E * cs[i]->Vp;
+        CK(cudaMemcpyAsync(cs[i]->f[cs[i]->cur], backup[i], n * sizeof(T), cudaMemcpyDeviceToDevice, st));
+      }
+      CK(cudaStreamSynchronize(st));
+      return 0;
+    };
+    // ms per step of the current configuration (one untimed step first)
+    auto trial = [&](double* per) -> int {
+      TRY(upload_ctrls(steps + 1, 0.0));
+      TRY(enqueue_step(L, st));
+      CK(cudaEventRecord(ev0, st));
+      for (int k = 0; k < steps; ++k) TRY(enqueue_step(L, st));
+      CK(cudaEventRecord(ev1, st));
+      float ms = 0.f;
+      CK(cudaEventSynchronize(ev1));
+      CK(cudaEventElapsedTime(&ms, ev0, ev1));
+      *per = ms / std::max(steps, 1);
+      return restore();
+    };
+    const int ebs[2] = {64, 128}, upcs[4] = {2, 4, 8, 16}, rws[3] = {1, 2, 4};
+    double best = 1e300;
+    int beb = fixed_eb > 0 ? fixed_eb : 128, bupc = fixed_upc > 0 ? fixed_upc : 8;
+    for (int ie = 0; ie < 2 && rc == 0; ++ie) {
+      if (fixed_eb > 0 && ebs[ie] != fixed_eb) continue;
+      for (int iu = 0; iu < 4 && rc == 0; ++iu) {
+        if (fixed_upc > 0 && upcs[iu] != fixed_upc) continue;
+        rc = configure(ebs[ie], upcs[iu]);
+        if (rc == DGBGK_EUNSUP) {  // shape does not fit: skip it
+          rc = 0;
+          continue;
+        }
+        double per = 0;
+        if (rc == 0) rc = trial(&per);
+        if (rc == 0) {
+          tune_ms[ie * 4 + iu] = per;
+          if (per < best) {
+            best = per;
+            beb = ebs[ie];
+            bupc = upcs[iu];
+          }
+        }
+      }
+    }
+    // then the moment kernel's rows per warp step for the chosen sweep shape
+    int brows = 0;
+    best = 1e300;
+    for (int ir = 0; ir < 3 && rc == 0; ++ir) {
+      rows = rws[ir];
+      rc = configure(beb, bupc);
+      if (rc == DGBGK_EUNSUP) {
+        rc = 0;
+        continue;
+      }
+      double per = 0;
+      if (rc == 0) rc = trial(&per);
+      if (rc == 0) {
+        tune_ms[8 + ir] = per;
+        if (per < best) {
+          best = per;
+          brows = rws[ir];
+        }
+      }
+    }
+    rows = brows;
+    for (T* p : backup) dfree(p);
+    TRY(rc);
+    return configure(beb, bupc);
+  }
+
+  int build_graph() {
+    if (gexec) return 0;
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    int rc = 0;
+    for (int k = 0; k < GRAPH_STEPS && rc == 0; ++k) rc = enqueue_step(L, st);
+    cudaError_t e = cudaStreamEndCapture(st, &g);
+    if (rc != 0) return rc;
+    CK(e);
+    CK(cudaGraphInstantiate(&gexec, g, 0));
+    cudaGraphDestroy(g);
+    return 0;
+  }
+
+  int advance(int max_steps, double tol, int* steps, double* l2) override {
+    if (max_steps < 0) {
+      set_error("max_steps < 0");
+      return DGBGK_EINVAL;
+    }
+    CK(cudaSetDevice(device));
+    bool rebuilt = false;
+    for (auto* c : cs)
+      if (c->hist_cap < max_steps) {
+        TRY(c->ensure_hist(max_steps));
+        rebuilt = true;
+      }
+    if (rebuilt) TRY(configure(eb, upc));
+    for (auto* c : cs) CK(cudaStreamSynchronize(c->st));
+    TRY(build_graph());
+    TRY(upload_ctrls(max_steps, tol));
+    CK(cudaEventRecord(ev0, st));
+    const int launches = max_steps > 0 ? (max_steps + GRAPH_STEPS - 1) / GRAPH_STEPS : 0;
+    const int chunk = 32;
+    int issued = 0, chunks = 0;
+    bool stop = false;
+    while (issued < launches && !stop) {
+      const int n = std::min(chunk, launches - issued);
+      for (int i = 0; i < n; ++i) CK(cudaGraphLaunch(gexec, st));
+      issued += n;
+      k_all_done<T><<<1, 256, 0, st>>>(L.args, d_done);
+      CK(cudaGetLastError());
+      CK(cudaMemcpyAsync(&h_done[chunks & 1], d_done, sizeof(int), cudaMemcpyDeviceToHost, st));
+      CK(cudaEventRecord(evp[chunks & 1], st));
+      ++chunks;
+      if (chunks >= 2) {  // look at the chunk before the one just issued
+        CK(cudaEventSynchronize(evp[chunks & 1]));
+        if (h_done[chunks & 1]) stop = true;
+      }
+    }
+    CK(cudaEventRecord(ev1, st));
+    CK(cudaStreamSynchronize(st));
+    CK(cudaEventElapsedTime(&last_ms, ev0, ev1));
+    int rc = 0;
+    for (size_t i = 0; i < cs.size(); ++i) {
+      Impl<T>* c = cs[i];
+      CK(cudaMemcpy(&c->hctrl[1], c->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost));
+      int ns = 0;
+      const int r = c->collect(c->hctrl[1], &ns, nullptr, nullptr, nullptr);
+      if (r != 0 && rc == 0) rc = r;
+      if (steps) steps[i] = ns;
+      if (l2) {
+        l2[i] = 0.0;
+        if (ns > 0) CK(cudaMemcpy(&l2[i], c->hist_l2 + ns - 1, sizeof(double), cudaMemcpyDeviceToHost));
+      }
+    }
+    return rc;
+  }
+
+  void info(int* o) const override {
+    o[0] = (int)cs.size();
+    o[1] = eb;
+    o[2] = upc;
+    o[3] = L.total_units;
+    o[4] = L.sweep_grid;
+    o[5] = L.mom_grid;
+    o[6] = L.mom_rows;
+  }
+  int tuning(int n, double* ms) const override {
+    for (int i = 0; i < n && i < (int)tune_ms.size(); ++i) ms[i] = tune_ms[i];
+    return 0;
+  }
+};
+
+}  // namespace
+
+struct dgbgk_batch {
+  std::unique_ptr<BatchBase> impl;
+};
+
+extern "C" {
+
+void dgbgk_batch_default_params(dgbgk_batch_params* p) {
+  if (!p) return;
+  p->tile_elems = 0;
+  p->units_per_cta = 0;
+  p->tune_steps = 4;
+}
+
+int dgbgk_batch_create(dgbgk_handle* const* cases, int ncases, const dgbgk_batch_params* prm,
+                       dgbgk_batch** out) {
+  if (!cases || ncases < 1 || !out) {
+    set_error("dgbgk_batch_create: no cases");
+    return DGBGK_EINVAL;
+  }
+  *out = nullptr;
+  dgbgk_batch_params p;
+  dgbgk_batch_default_params(&p);
+  if (prm) p = *prm;
+  const int prec = cases[0] && cases[0]->impl ? cases[0]->impl->prec : 0;
+  for (int i = 0; i < ncases; ++i)
+    if (!cases[i] || !cases[i]->impl || cases[i]->impl->prec != prec) {
+      set_error("dgbgk_batch_create: NULL handle or mixed precision");
+      return DGBGK_EINVAL;
+    }
+  for (int i = 0; i < ncases; ++i)
+    for (int k = 0; k < i; ++k)
+      if (cases[i] == cases[k]) {
+        set_error("dgbgk_batch_create: a handle appears twice");
+        return DGBGK_EINVAL;
+      }
+  std::unique_ptr<BatchBase> b;
+  int rc = 0;
+  if (prec == 64) {
+    auto* bi = new BatchImpl<double>();
+    b.reset(bi);
+    std::vector<Impl<double>*> v;
+    for (int i = 0; i < ncases; ++i) v.push_back(static_cast<Impl<double>*>(cases[i]->impl.get()));
+    rc = bi->init(v);
+    if (rc == 0) rc = bi->autotune(p.tile_elems, p.units_per_cta, std::max(1, p.tune_steps));
+  } else {
+    auto* bi = new BatchImpl<float>();
+    b.reset(bi);
+    std::vector<Impl<float>*> v;
+    for (int i = 0; i < ncases; ++i) v.push_back(static_cast<Impl<float>*>(cases[i]->impl.get()));
+    rc = bi->init(v);
+    if (rc == 0) rc = bi->autotune(p.tile_elems, p.units_per_cta, std::max(1, p.tune_steps));
+  }
+  if (rc != 0) return rc;
+  *out = new dgbgk_batch{std::move(b)};
+  return DGBGK_OK;
+}
+
+int dgbgk_batch_advance(dgbgk_batch* b, int max_steps, double tol, int* steps_done, double* res_l2_last) {
+  if (!b || !b->impl) return set_error("NULL batch"), DGBGK_EINVAL;
+  return b->impl->advance(max_steps, tol, steps_done, res_l2_last);
+}
+
+int dgbgk_batch_info(const dgbgk_batch* b, int* out) {
+  if (!b || !b->impl || !out) return set_error("NULL batch"), DGBGK_EINVAL;
+  b->impl->info(out);
+  return DGBGK_OK;
+}
+
+int dgbgk_batch_tuning(const dgbgk_batch* b, int n, double* ms_per_step) {
+  if (!b || !b->impl || !ms_per_step) return set_error("NULL batch"), DGBGK_EINVAL;
+  return b->impl->tuning(n, ms_per_step);
+}
+
+int dgbgk_batch_last_timing(const dgbgk_batch* b, double* total_ms) {
+  if (!b || !b->impl || !total_ms) return set_error("NULL batch"), DGBGK_EINVAL;
+  *total_ms = b->impl->last_ms;
+  return DGBGK_OK;
+}
+
+void dgbgk_batch_destroy(dgbgk_batch* b) { delete b; }
 
 }  // extern "C"
 

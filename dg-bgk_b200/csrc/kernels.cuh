@@ -6,8 +6,8 @@
 //               (src/gteqnf.f90:315-326).  Persistent warps take R whole
 //               velocity rows of f at a time (32/R lanes per row) from a
 //               per-warp ring of stages filled by 1-D bulk copies, so f is
-//               read from HBM once for both passes; the velocity tables sit
-//               in shared memory and every access is a 16-byte vector.
+//               read from HBM once for both passes; every access is a
+//               16-byte vector.
 //   k_wall    : FLUCON2 (src/flucon2.f90:134-233), one warp per wall side.
 //   k_sweep   : the whole velocity-loop body (GTEQNF, GETFLA, GETELC,
 //               EDGFLXOPT/GETBOU, GETINC/CMMINC, ADTHEM, INFLOW;
@@ -110,21 +110,74 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t b
                : "memory");
 }
 
-// ------------------------------------------------------------ moments ----
-template <class T> struct MomArgs {
-  const T* __restrict__ f;
-  const T* __restrict__ tabs;  // [3][Vp] cx, cy, WEIGHT*JAC*FRAC, zero past V
-  ElemRec<T>* __restrict__ rec;
-  double* __restrict__ nraw;   // INT (number density before the 1e-20 test)
-  double* __restrict__ disux;
-  double* __restrict__ disuy;
-  double* __restrict__ disps;
-  double* __restrict__ mu;
+// -------------------------------------------------------------- cases ----
+// One case (a mesh, its velocity grid and its state) as the kernels see it.
+// Every launch works on a table of cases: a single handle is a table of one,
+// a batch a table of many.  The work of the launch set is flattened: sweep
+// units, moment row groups and wall sides of case c are [off[c], off[c+1]).
+template <class T> struct alignas(64) CaseDev {
+  CUtensorMap tm[2];  // f[b] as [3E rows][Vp] (sweep tile boxes, 64-byte swizzle)
+  T* f[2];            // state, ping-pong; Ctrl::cur is the current one
+  ElemRec<T>* rec;
+  const int* halo_off;
+  const int* halo_list;
+  const T* cx;     // [Vp] sweep tables, zero past V
+  const T* cy;
+  const T* nfinf;
+  const T* tabs;   // [3][Vp] cx, cy, WEIGHT*JAC*FRAC for the moments, zero past V
+  const T* bTw;    // per boundary side: wall temperature, wall velocity (x, y), ETA
+  const T* bUw;
+  T* bEta;
+  double* bEtaD;
+  const double* cxD;  // [V] FP64 velocity tables for FLUCON2
+  const double* cyD;
+  const double* wjf;
+  const WallSide* walls;
+  const T* cmax;   // IMMAT = 0 residual tables
+  const T* cmin;
+  double* nraw;    // per DG node: INT (number density before the 1e-20 test)
+  double* disux;
+  double* disuy;
+  double* disps;
+  double* mu;
+  double* hist_linf;  // per step of an advance call
+  double* hist_l2;
+  double* hist_dt;
   Ctrl* ctrl;
-  int ndg, V, Vp, nstage;
+  double MM, sigt;  // M/NA, PI*d*d
+  T alpha, rgas;
+  int E, V, Vp, nblocks, nvt, tpu;
+  int nwall;          // FLUCON2 wall sides
   unsigned rowbytes;  // V*sizeof(T) rounded up to 16
-  double MM, sigt;    // M/NA, PI*d*d
 };
+
+template <class T> struct BatchArgs {
+  const CaseDev<T>* cases;  // [ncases]
+  const int* unit_off;      // [ncases + 1] sweep work units
+  const int* grp_off;       // [ncases + 1] moment row groups
+  const int* wall_off;      // [ncases + 1] wall sides
+  BatchCtl* ctl;
+  int ncases;
+  int max_halo;             // over the cases (sweep tile layout)
+  int mom_stages;           // moment ring stages per warp
+  unsigned mom_rowbytes;    // moment ring row size (max over the cases)
+};
+
+// The case c with off[c] <= x < off[c + 1] (cases with empty ranges are
+// skipped: the largest c with off[c] <= x).
+__device__ __forceinline__ int find_case(const int* __restrict__ off, int n, int x) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (off[mid] <= x)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+// ------------------------------------------------------------ moments ----
 
 // sqrt by a reciprocal-square-root seed and one Newton step for 1/sqrt(x),
 // y <- y (3 - x y^2)/2, in FP64 (relative error ~1e-14 from a ~1e-7 seed).
@@ -225,48 +278,68 @@ template <int L> __device__ __forceinline__ double group_sum(double v) {
   return v;
 }
 
-// Moment kernel: persistent warps; each warp takes R DG nodes (velocity rows)
-// at a time, L = 32/R lanes per row, from a per-warp ring of stages filled by
-// 1-D bulk copies, so f is read from HBM once for both passes and the R
-// rows' reductions and FP64 epilogues run side by side.
-template <class T, int R>
-__global__ void __launch_bounds__(512, 1) k_moments(MomArgs<T> a) {
-  if (a.ctrl->done) return;
+// Moment kernel: persistent warps over the flattened row groups of all the
+// cases; each warp takes R DG nodes (velocity rows) at a time, L = 32/R
+// lanes per row, from a per-warp ring of stages filled by 1-D bulk copies,
+// so f is read from HBM once for both passes.  ONE: a single case, passed
+// as a kernel parameter, with its velocity tables staged in shared memory;
+// otherwise the case table, with the tables read through L1 (they differ
+// from case to case).  MU's maximum goes to the case's control block once
+// per warp and case.
+template <class T, int R, bool ONE>
+__global__ void __launch_bounds__(512, 1)
+    k_moments(BatchArgs<T> a, int total_groups, const __grid_constant__ CaseDev<T> one) {
   constexpr int L = 32 / R;
   extern __shared__ __align__(128) unsigned char sm_raw[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
   const int grp = lane / L, sub = lane % L;
-  // layout: [barriers][tables 3*Vp][rings: warp, stage, R rows]
-  uint64_t* bars = reinterpret_cast<uint64_t*>(sm_raw) + warp * a.nstage;
-  T* tb = reinterpret_cast<T*>(sm_raw + 128 * ((nwarp * a.nstage * 8 + 127) / 128));
-  const size_t stage_bytes = (size_t)R * a.rowbytes;
-  unsigned char* ring =
-      reinterpret_cast<unsigned char*>(tb + 3 * (size_t)a.Vp) + (size_t)warp * a.nstage * stage_bytes;
-  for (int i = threadIdx.x; i < 3 * a.Vp; i += blockDim.x) tb[i] = a.tabs[i];
-  const int ngroups = (a.ndg + R - 1) / R;
+  const int nstage = a.mom_stages;
+  // layout: [barriers][tables [3][Vp] (ONE)][rings: warp, stage, R rows]
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sm_raw) + warp * nstage;
+  T* tb1 = reinterpret_cast<T*>(sm_raw + 128 * (((size_t)nwarp * nstage * 8 + 127) / 128));
+  const size_t tbytes = ONE ? (3 * (size_t)one.Vp * sizeof(T) + 127) / 128 * 128 : 0;
+  const size_t stage_bytes = (size_t)R * a.mom_rowbytes;
+  unsigned char* ring = reinterpret_cast<unsigned char*>(tb1) + tbytes + (size_t)warp * nstage * stage_bytes;
+  if (ONE)
+    for (int i = threadIdx.x; i < 3 * one.Vp; i += blockDim.x) tb1[i] = one.tabs[i];
   const int gw = blockIdx.x * nwarp + warp, stride = gridDim.x * nwarp;
   if (lane == 0) {
-    for (int s = 0; s < a.nstage; ++s) mbar_init(&bars[s], 1);
+    for (int s = 0; s < nstage; ++s) mbar_init(&bars[s], 1);
     fence_mbar_init();
   }
   __syncthreads();
-  // lane 0: the rows of group g into stage s
+  // lane 0: the rows of group g into stage s (none when the case is done)
   auto fill = [&](int s, int g) {
-    const int r0 = g * R, nr = min(R, a.ndg - r0);
-    mbar_expect_tx(&bars[s], (unsigned)nr * a.rowbytes);
+    const int c = ONE ? 0 : find_case(a.grp_off, a.ncases, g);
+    const CaseDev<T>& C = ONE ? one : a.cases[c];
+    const Ctrl* ctl = C.ctrl;
+    const int r0 = (g - (ONE ? 0 : a.grp_off[c])) * R;
+    const int nr = ctl->done ? 0 : min(R, 3 * C.E - r0);
+    const T* f = C.f[ctl->cur];
+    mbar_expect_tx(&bars[s], (unsigned)nr * C.rowbytes);
     for (int k = 0; k < nr; ++k)
-      bulk_load(ring + (size_t)s * stage_bytes + (size_t)k * a.rowbytes, a.f + (size_t)(r0 + k) * a.Vp,
-                a.rowbytes, &bars[s]);
+      bulk_load(ring + (size_t)s * stage_bytes + (size_t)k * C.rowbytes, f + (size_t)(r0 + k) * C.Vp, C.rowbytes,
+                &bars[s]);
   };
   if (lane == 0)
-    for (int s = 0; s < a.nstage; ++s)
-      if (gw + s * stride < ngroups) fill(s, gw + s * stride);
-  const int nq = (int)(a.rowbytes / 16);
+    for (int s = 0; s < nstage; ++s)
+      if (gw + s * stride < total_groups) fill(s, gw + s * stride);
   uint32_t parity = 0;  // bit s: parity of stage s
   int s = 0;
   bool aborted = false;
+  int mu_case = -1;
   double mumax = 0.0;
-  for (int g = gw; g < ngroups; g += stride) {
+  // MU >= 0: the max of the bit patterns is the max of the values
+  auto flush_mu = [&]() {
+    const double m = warp_max(mumax);
+    if (lane == 0 && mu_case >= 0 && m > 0.0)
+      atomicMax(reinterpret_cast<unsigned long long*>(&(ONE ? one : a.cases[mu_case]).ctrl->maxmu),
+                (unsigned long long)__double_as_longlong(m));
+    mumax = 0.0;
+  };
+  int c = 0;
+  for (int g = gw; g < total_groups; g += stride) {
+    c = ONE ? 0 : find_case(a.grp_off, a.ncases, g);  // warp-uniform
     int ok = 1;
     if (lane == 0) ok = mbar_wait_bounded(&bars[s], (parity >> s) & 1) ? 1 : 0;
     ok = __shfl_sync(0xffffffffu, ok, 0);
@@ -276,12 +349,18 @@ __global__ void __launch_bounds__(512, 1) k_moments(MomArgs<T> a) {
     }
     mbar_wait_bounded(&bars[s], (parity >> s) & 1);  // completed: returns at once
     parity ^= 1u << s;
-    const int node = g * R + grp;
-    const bool live = node < a.ndg;
-    const T* row = reinterpret_cast<const T*>(ring + (size_t)s * stage_bytes + (size_t)grp * a.rowbytes);
-    const int nql = live ? nq : 0;
+    const CaseDev<T>& C = ONE ? one : a.cases[c];
+    if (c != mu_case) {
+      flush_mu();
+      mu_case = c;
+    }
+    const int node = (g - (ONE ? 0 : a.grp_off[c])) * R + grp;
+    const T* tb = ONE ? tb1 : C.tabs;
+    const bool live = !C.ctrl->done && node < 3 * C.E;
+    const T* row = reinterpret_cast<const T*>(ring + (size_t)s * stage_bytes + (size_t)grp * C.rowbytes);
+    const int nql = live ? (int)(C.rowbytes / 16) : 0;
     double s0 = 0, s1 = 0, s2 = 0;
-    RowMath<T>::pass1(row, tb, a.Vp, nql, sub, L, s0, s1, s2);
+    RowMath<T>::pass1(row, tb, C.Vp, nql, sub, L, s0, s1, s2);
     s0 = group_sum<L>(s0);
     s1 = group_sum<L>(s1);
     s2 = group_sum<L>(s2);
@@ -292,26 +371,26 @@ __global__ void __launch_bounds__(512, 1) k_moments(MomArgs<T> a) {
       uy = s2 / s0;
     }
     double sp = 0, sc = 0;
-    RowMath<T>::pass2(row, tb, a.Vp, nql, sub, L, ux, uy, sp, sc);
+    RowMath<T>::pass2(row, tb, C.Vp, nql, sub, L, ux, uy, sp, sc);
     sp = group_sum<L>(sp);
     sc = group_sum<L>(sc);
     __syncwarp();
     // the rows are consumed: refill this stage with the group nstage ahead
     if (lane == 0) {
-      const int nxt = g + a.nstage * stride;
-      if (nxt < ngroups) {
+      const int nxt = g + nstage * stride;
+      if (nxt < total_groups) {
         fence_proxy_async_smem();
         fill(s, nxt);
       }
     }
     if (sub == 0 && live) {
-      const double ps = sp * a.MM;
+      const double ps = sp * C.MM;
       const double ct = (nd >= TINY_D) ? sc / nd : 0.0;
-      const double mu = sqrt(2.0) * ct * a.sigt * nd;
+      const double mu = sqrt(2.0) * ct * C.sigt * nd;
       const int e = node / 3, i = node - 3 * (node / 3);
-      ElemRec<T>& en = a.rec[e];
+      ElemRec<T>& en = C.rec[e];
       if (ps >= TINY_D) {  // GTEQNF (src/gteqnf.f90:317-326)
-        const double rho = a.MM * nd;
+        const double rho = C.MM * nd;
         const double b2 = rho / (2 * ps);
         en.A[i] = (T)(nd * (b2 / PI_D));
         en.ex[i] = (T)(sizeof(T) == 4 ? -b2 * LOG2E_D : -b2);
@@ -322,85 +401,51 @@ __global__ void __launch_bounds__(512, 1) k_moments(MomArgs<T> a) {
       en.ux[i] = (T)ux;
       en.uy[i] = (T)uy;
       en.mu[i] = (T)mu;
-      a.nraw[node] = s0;
-      a.disux[node] = ux;
-      a.disuy[node] = uy;
-      a.disps[node] = ps;
-      a.mu[node] = mu;
+      C.nraw[node] = s0;
+      C.disux[node] = ux;
+      C.disuy[node] = uy;
+      C.disps[node] = ps;
+      C.mu[node] = mu;
       mumax = fmax(mumax, mu);
     }
-    s = (s + 1 == a.nstage) ? 0 : s + 1;
+    s = (s + 1 == nstage) ? 0 : s + 1;
   }
   if (aborted) {
     if (lane == 0) {
-      a.ctrl->timeout = 1;
-      for (int k = 0; k < a.nstage; ++k) mbar_wait_bounded(&bars[k], (parity >> k) & 1);
+      (ONE ? one : a.cases[c]).ctrl->timeout = 1;
+      for (int k = 0; k < nstage; ++k) mbar_wait_bounded(&bars[k], (parity >> k) & 1);
     }
     return;
   }
-  // MU >= 0: the max of the bit patterns is the max of the values
-  mumax = warp_max(mumax);
-  if (lane == 0 && mumax > 0.0)
-    atomicMax(reinterpret_cast<unsigned long long*>(&a.ctrl->maxmu), (unsigned long long)__double_as_longlong(mumax));
+  flush_mu();
 }
 
 // --------------------------------------------------------- wall flux ----
-template <class T> struct WallArgs {
-  const T* __restrict__ f;
-  const WallSide* __restrict__ walls;
-  const double* __restrict__ cx;
-  const double* __restrict__ cy;
-  const double* __restrict__ wjf;
-  T* __restrict__ beta_t;   // ETA per boundary side (sweep precision)
-  double* __restrict__ beta_d;
-  Ctrl* ctrl;
-  int nwall, V, Vp;
-};
-
-template <class T> __global__ void __launch_bounds__(256) k_wall(WallArgs<T> a) {
-  if (a.ctrl->done) return;
+// FLUCON2 (src/flucon2.f90:134-233): one warp per wall side of any case.
+template <class T> __global__ void __launch_bounds__(256) k_wall(BatchArgs<T> a, int total_walls) {
   const int w = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
-  if (w >= a.nwall) return;
-  const WallSide ws = a.walls[w];
-  const T* f1 = a.f + ((size_t)ws.elem * 3 + ws.in1) * a.Vp;
-  const T* f2 = a.f + ((size_t)ws.elem * 3 + ws.in2) * a.Vp;
+  if (w >= total_walls) return;
+  const int c = find_case(a.wall_off, a.ncases, w);
+  const CaseDev<T>& C = a.cases[c];
+  if (C.ctrl->done) return;
+  const WallSide ws = C.walls[w - a.wall_off[c]];
+  const T* f = C.f[C.ctrl->cur];
+  const T* f1 = f + ((size_t)ws.elem * 3 + ws.in1) * C.Vp;
+  const T* f2 = f + ((size_t)ws.elem * 3 + ws.in2) * C.Vp;
   double s = 0;
-  for (int v = lane; v < a.V; v += 32) {
-    const double test = a.cx[v] * ws.anx + a.cy[v] * ws.any;
-    if (test > 0.0) s += fabs(test) * (0.5 * ((double)f1[v] + (double)f2[v])) * a.wjf[v];
+  for (int v = lane; v < C.V; v += 32) {
+    const double test = C.cxD[v] * ws.anx + C.cyD[v] * ws.any;
+    if (test > 0.0) s += fabs(test) * (0.5 * ((double)f1[v] + (double)f2[v])) * C.wjf[v];
   }
   s = warp_sum(s);
   if (lane == 0) {
     const double eta = s / ws.sumbottom;
-    a.beta_d[ws.bside] = eta;
-    a.beta_t[ws.bside] = (T)eta;
+    C.bEtaD[ws.bside] = eta;
+    C.bEta[ws.bside] = (T)eta;
   }
 }
 
 // -------------------------------------------------------------- sweep ----
-template <class T> struct SweepArgs {
-  const T* __restrict__ fin;
-  T* __restrict__ fout;
-  const ElemRec<T>* __restrict__ rec;
-  const int* __restrict__ halo_off;
-  const int* __restrict__ halo_list;
-  const T* __restrict__ cx;     // [Vp], zero past V
-  const T* __restrict__ cy;     // [Vp], zero past V
-  const T* __restrict__ nfinf;  // [Vp], zero past V
-  const T* __restrict__ bTw;
-  const T* __restrict__ bUw;
-  const T* __restrict__ bEta;
-  const T* __restrict__ cmax;  // IMMAT = 0 only
-  const T* __restrict__ cmin;
-  double* __restrict__ part_max;
-  double* __restrict__ part_sq;
-  Ctrl* ctrl;
-  int E, V, Vp, nblocks, max_halo;
-  int nvt;  // velocity tiles holding some v < V
-  int tpu;  // velocity tiles per work unit (<= SweepGeo::TPU_MAX)
-  T alpha, rgas;
-};
-
 // DTE = min(CSAFE/maxMU, DTEc)  (src/alotim2.f90:10-15, src/advnce.f90:258-262)
 __device__ __forceinline__ double step_dt(const Ctrl* c) {
   const double mx = c->maxmu;
@@ -581,14 +626,14 @@ __device__ __forceinline__ void sweep_p1(const ElemRec<T>& r, unsigned char* tl,
 //    length, inflow and wall sides read the element itself), the wall sides'
 //    fluxes (GETBOU src/getbou.f90:142-281), GETINC/CMMINC, ADTHEM and INFLOW;
 //    16-byte vector stores of the new rows.
+// ONE: a single case passed as a kernel parameter (its fields come from the
+// constant bank, no registers); otherwise the case table.
 // Upwinding: the own value is taken where SC = n.c > 0.  The reference takes
 // it where SC > 0 for the ISIDE(3) element and SC >= 0 for the other; the
 // two differ only at SC = 0, where the flux SC*value is zero either way.
-template <class T, int EB, int IMMAT>
+template <class T, int EB, int IMMAT, bool ONE>
 __global__ void __launch_bounds__(2 * EB, sizeof(T) == 4 ? 2 : 1)
-    k_sweep(const __grid_constant__ CUtensorMap tm_in, const __grid_constant__ CUtensorMap tm_out,
-            SweepArgs<T> a) {
-  if (a.ctrl->done) return;
+    k_sweep(BatchArgs<T> a, int total_units, const __grid_constant__ CaseDev<T> one) {
   using G = SweepGeo<T>;
   using VO = Vec<T>;
   using VecT = typename VO::type;
@@ -610,13 +655,8 @@ __global__ void __launch_bounds__(2 * EB, sizeof(T) == 4 ? 2 : 1)
   T* const vtab = reinterpret_cast<T*>(hrec + (size_t)a.max_halo * HR);  // cx, cy, NFINF
   constexpr int UV = G::TPU_MAX * VT;
   int* const hl = reinterpret_cast<int*>(vtab + 3 * UV);  // halo elements of the unit's block
-  const int nvg = (a.nvt + a.tpu - 1) / a.tpu;
-  const int nunits = a.nblocks * nvg;
   const int j = tid < EB ? tid : tid - EB, hh = tid < EB ? 0 : 1;
-
-  const double dtd = step_dt(a.ctrl);
-  const T dt = (T)dtd, dth = (T)(0.5 * dtd), dth3 = (T)(0.5 * dtd / 3.0), third = (T)(1.0 / 3.0);
-  double rmax = 0.0, rsq = 0.0;
+  const T third = (T)(1.0 / 3.0);
   if (tid == 0) {
     mbar_init(&bars[0], 1);
     mbar_init(&bars[1], 1);
@@ -626,382 +666,376 @@ __global__ void __launch_bounds__(2 * EB, sizeof(T) == 4 ? 2 : 1)
   uint32_t par = 0;  // bit b: parity of the next phase of bars[b]
   bool aborted = false;
   int abort_buf = 0;
+  // the new block rows of tile vt (written into buffer bi by every thread,
+  // each followed by a proxy fence, before a barrier) as NBOX box stores
+  // issued by thread 0; rows past 3E are not written
+  auto store = [&](const CUtensorMap* map, int vt, int bi, int y0) {
+    const unsigned char* srcb = base + (size_t)bi * tile_bytes;
+#pragma unroll
+    for (int x = 0; x < NBOX; ++x) tma_store_2d(map, vt * VT, y0 + x * G::BOX_ROWS, srcb + x * BOX_BYTES);
+    bulk_commit();
+  };
 
-  int unit = blockIdx.x;
+  int unit = blockIdx.x, c = 0;
   // the unit after this one, drawn ahead so the atomic's latency is hidden
-  int next = (tid == 0 && unit < nunits) ? (int)gridDim.x + atomicAdd(&a.ctrl->sweep_next, 1) : 0;
-  while (unit < nunits) {
-    const int b = unit % a.nblocks, vg = unit / a.nblocks;
-    const int e0 = b * EB, nb = min(EB, a.E - e0);
-    const int h0 = a.halo_off[b], nh = a.halo_off[b + 1] - h0;
-    const int vt0 = vg * a.tpu, ntl = min(a.tpu, a.nvt - vt0);
+  int next = (tid == 0 && unit < total_units) ? (int)gridDim.x + atomicAdd(&a.ctl->sweep_next, 1) : 0;
+  while (unit < total_units) {
+    c = ONE ? 0 : find_case(a.unit_off, a.ncases, unit);
+    const CaseDev<T>& C = ONE ? one : a.cases[c];
+    const bool active = !C.ctrl->done;  // the same for every thread
+    const CUtensorMap* last_map = nullptr;
+    int last_vt = 0, last_bi = 0, last_y0 = 0;
+    if (active) {
+      const int lu = unit - (ONE ? 0 : a.unit_off[c]);
+      const int b = lu % C.nblocks, vg = lu / C.nblocks;
+      const int e0 = b * EB, nb = min(EB, C.E - e0);
+      const int h0 = C.halo_off[b], nh = C.halo_off[b + 1] - h0;
+      const int vt0 = vg * C.tpu, ntl = min(C.tpu, C.nvt - vt0);
+      const int cur = C.ctrl->cur;
+      const double dtd = step_dt(C.ctrl);
+      const T dt = (T)dtd, dth = (T)(0.5 * dtd), dth3 = (T)(0.5 * dtd / 3.0);
+      double rmax = 0.0, rsq = 0.0;
 
-    // unit prologue: block records and halo record heads (cp.async, completed
-    // with the first tile's group), the halo list and the velocity tables
-    {
-      const uint4* src = reinterpret_cast<const uint4*>(a.rec + e0);
-      for (int w = tid; w < nb * RW; w += NT) cp_async16(reinterpret_cast<uint4*>(recs) + w, src + w);
-      const int* __restrict__ hlist = a.halo_list + h0;
-      for (int w = tid; w < nh * HW; w += NT) {
-        const int s = w / HW, k = w - s * HW;
-        cp_async16(hrec + (size_t)s * HR + 16 * k, reinterpret_cast<const uint4*>(a.rec + hlist[s]) + k);
-      }
-      for (int s = tid; s < nh; s += NT) hl[s] = hlist[s];
-      const int v0 = vt0 * VT;
-      for (int v = tid; v < ntl * VT; v += NT) {
-        vtab[v] = a.cx[v0 + v];
-        vtab[UV + v] = a.cy[v0 + v];
-        vtab[2 * UV + v] = a.nfinf[v0 + v];
-      }
-    }
-    // the rows of tile vt: work item (s, i, half) copies 32 contiguous bytes
-    // of row i of block element s (s < nb, slot s) or halo element s - nb
-    // (slot EB + s - nb)
-    // copies of tile vt into buffer bi: the block's rows (3*e0 ..) as NBOX
-    // TMA boxes issued by thread 0 once the buffer's last box store has
-    // read it (rows past 3E read as zeros), the halo rows by cp.async, four
-    // threads per 64-byte row
-    auto issue = [&](int vt, int bi) {
-      unsigned char* dst = base + (size_t)bi * tile_bytes;
-      if (tid == 0) {
-        bulk_wait_read0();
-        fence_proxy_async_smem();  // the buffer's previous generic accesses
-        mbar_expect_tx(&bars[bi], NBOX * BOX_BYTES);
-#pragma unroll
-        for (int x = 0; x < NBOX; ++x)
-          tma_load_2d(dst + x * BOX_BYTES, &tm_in, vt * VT, 3 * e0 + x * G::BOX_ROWS, &bars[bi]);
-      }
-      const T* src = a.fin + (size_t)vt * VT;
-      for (int w = tid; w < nh * 12; w += NT) {
-        const int h = w / 12, rr = w - 12 * h, i = rr >> 2, c = rr & 3;
-        cp_async16(dst + tile_off(3 * (EB + h) + i, c), src + ((size_t)hl[h] * 3 + i) * a.Vp + c * W);
-      }
-    };
-    // the new block rows of tile vt (written into buffer bi by every thread,
-    // each followed by a proxy fence, before a barrier) as NBOX box stores
-    // issued by thread 0; rows past 3E are not written
-    auto store = [&](int vt, int bi) {
-      const unsigned char* srcb = base + (size_t)bi * tile_bytes;
-#pragma unroll
-      for (int x = 0; x < NBOX; ++x) tma_store_2d(&tm_out, vt * VT, 3 * e0 + x * G::BOX_ROWS, srcb + x * BOX_BYTES);
-      bulk_commit();
-    };
-    __syncthreads();  // hl
-    issue(vt0, 0);
-    cp_async_commit();
-
-    for (int k = 0; k < ntl; ++k) {
-      const int bi = k & 1;
-      unsigned char* const tl = base + (size_t)bi * tile_bytes;
-      // thread 0 waits for the boxes (the others wait in the barrier, not
-      // spinning); every thread waits for its own halo copies
-      const uint32_t ph = (par >> bi) & 1u;
-      const bool ok = tid != 0 || mbar_wait_bounded(&bars[bi], ph);
-      par ^= 1u << bi;
-      cp_async_wait<0>();
-      // tile k has landed (or the wait expired), and every thread has written
-      // and fenced its new rows of tile k - 1
-      if (__syncthreads_or(ok ? 0 : 1)) {
-        aborted = true;
-        abort_buf = bi;
-        break;
-      }
-      if (tid != 0) mbar_try_wait(&bars[bi], ph);  // completed: acquires the box data
-      if (tid == 0 && k > 0) store(vt0 + k - 1, bi ^ 1);
-      const int vb0 = (vt0 + k) * VT;
-      const T* vx = vtab + k * VT;
-      const T* vy = vtab + UV + k * VT;
-      const T* vn = vtab + 2 * UV + k * VT;
-
-      // ---- phase 1: block element j (half hh), then the halo chunk by chunk
-      VecT qr[2][3], ur[2];
-      if (j < nb) {
-        const ElemRec<T>& r = recs[j];
-#pragma unroll
-        for (int cc = 0; cc < 2; ++cc) {
-          const int c = 2 * hh + cc;
-          sweep_p1<T>(r, tl, 3 * j, c, vld<T>(vx + c * W), vld<T>(vy + c * W), dth, dth3, qr[cc], ur[cc]);
+      // unit prologue: block records and halo record heads (cp.async,
+      // completed with the first tile's group), the halo list and the
+      // velocity tables
+      {
+        const uint4* src = reinterpret_cast<const uint4*>(C.rec + e0);
+        for (int w = tid; w < nb * RW; w += NT) cp_async16(reinterpret_cast<uint4*>(recs) + w, src + w);
+        const int* __restrict__ hlist = C.halo_list + h0;
+        for (int w = tid; w < nh * HW; w += NT) {
+          const int s = w / HW, k = w - s * HW;
+          cp_async16(hrec + (size_t)s * HR + 16 * k, reinterpret_cast<const uint4*>(C.rec + hlist[s]) + k);
+        }
+        for (int s = tid; s < nh; s += NT) hl[s] = hlist[s];
+        const int v0 = vt0 * VT;
+        for (int v = tid; v < ntl * VT; v += NT) {
+          vtab[v] = C.cx[v0 + v];
+          vtab[UV + v] = C.cy[v0 + v];
+          vtab[2 * UV + v] = C.nfinf[v0 + v];
         }
       }
-      for (int w = tid; w < nh * NCH; w += NT) {
-        const int hs = w >> 2, c = w & 3;
-        const ElemRec<T>& r = *reinterpret_cast<const ElemRec<T>*>(hrec + (size_t)hs * HR);
-        VecT qd[3], ud;
-        sweep_p1<T>(r, tl, 3 * (EB + hs), c, vld<T>(vx + c * W), vld<T>(vy + c * W), dth, dth3, qd, ud);
-      }
-      __syncthreads();
-      // the other buffer's tile k - 1 is stored (or being stored): load tile k + 1
-      if (k + 1 < ntl) {
-        issue(vt0 + k + 1, bi ^ 1);
-        cp_async_commit();
-      }
+      // copies of tile vt into buffer bi: the block's rows (3*e0 ..) as NBOX
+      // TMA boxes issued by thread 0 once the buffer's last box store has
+      // read it (rows past 3E read as zeros), the halo rows by cp.async, four
+      // threads per 64-byte row
+      auto issue = [&](int vt, int bi) {
+        unsigned char* dst = base + (size_t)bi * tile_bytes;
+        if (tid == 0) {
+          bulk_wait_read0();
+          fence_proxy_async_smem();  // the buffer's previous generic accesses
+          mbar_expect_tx(&bars[bi], NBOX * BOX_BYTES);
+#pragma unroll
+          for (int x = 0; x < NBOX; ++x)
+            tma_load_2d(dst + x * BOX_BYTES, &C.tm[cur], vt * VT, 3 * e0 + x * G::BOX_ROWS, &bars[bi]);
+        }
+        const T* src = C.f[cur] + (size_t)vt * VT;
+        for (int w = tid; w < nh * 12; w += NT) {
+          const int h = w / 12, rr = w - 12 * h, i = rr >> 2, cq = rr & 3;
+          cp_async16(dst + tile_off(3 * (EB + h) + i, cq), src + ((size_t)hl[h] * 3 + i) * C.Vp + cq * W);
+        }
+      };
+      __syncthreads();  // hl
+      issue(vt0, 0);
+      cp_async_commit();
 
-      // ---- phase 2: the update of block element j, half hh.  Row offsets
-      // are taken at chunk 2*hh; chunk 2*hh+1 of the same row is at offset ^ 16.
-      T rmt = (T)0, sqt = (T)0;
-      unsigned own[3];
+      for (int k = 0; k < ntl; ++k) {
+        const int bi = k & 1;
+        unsigned char* const tl = base + (size_t)bi * tile_bytes;
+        // thread 0 waits for the boxes (the others wait in the barrier, not
+        // spinning); every thread waits for its own halo copies
+        const uint32_t ph = (par >> bi) & 1u;
+        const bool ok = tid != 0 || mbar_wait_bounded(&bars[bi], ph);
+        par ^= 1u << bi;
+        cp_async_wait<0>();
+        // tile k has landed (or the wait expired), and every thread has
+        // written and fenced its new rows of tile k - 1
+        if (__syncthreads_or(ok ? 0 : 1)) {
+          aborted = true;
+          abort_buf = bi;
+          break;
+        }
+        if (tid != 0) mbar_try_wait(&bars[bi], ph);  // completed: acquires the box data
+        if (tid == 0 && k > 0) store(&C.tm[cur ^ 1], vt0 + k - 1, bi ^ 1, 3 * e0);
+        const int vb0 = (vt0 + k) * VT;
+        const T* vx = vtab + k * VT;
+        const T* vy = vtab + UV + k * VT;
+        const T* vn = vtab + 2 * UV + k * VT;
+
+        // ---- phase 1: block element j (half hh), then the halo chunk by chunk
+        VecT qr[2][3], ur[2];
+        if (j < nb) {
+          const ElemRec<T>& r = recs[j];
 #pragma unroll
-      for (int i = 0; i < 3; ++i) own[i] = tile_off(3 * j + i, 2 * hh);
-      VecT outv[2][3];
-      if (j < nb) {
-        const ElemRec<T>& r = recs[j];
-        const int e = e0 + j;
-        const T area3 = r.area * third;
-        T mudt[3], mmdt[3], cmx[3], cmn[3];
-#pragma unroll
-        for (int i = 0; i < 3; ++i) {
-          mudt[i] = r.mu[i] * dt;
-          mmdt[i] = r.mm[i] * dt;
-          if (IMMAT == 0) {
-            cmx[i] = a.cmax[3 * e + i];
-            cmn[i] = a.cmin[3 * e + i];
+          for (int cc = 0; cc < 2; ++cc) {
+            const int cq = 2 * hh + cc;
+            sweep_p1<T>(r, tl, 3 * j, cq, vld<T>(vx + cq * W), vld<T>(vy + cq * W), dth, dth3, qr[cc], ur[cc]);
           }
         }
-        // per edge: the flux source's rows and AL*n (zero on inflow and
-        // wall sides, whose flux the wall path adds)
-        unsigned srcp[3], srcq[3];
-        T anx[3], any[3];
-#pragma unroll
-        for (int k2 = 0; k2 < 3; ++k2) {
-          const int inf = r.edge[k2].info, kind = inf & 3;
-          const int r0 = 3 * (inf >> 8);
-          srcp[k2] = tile_off(r0 + ((inf >> 3) & 3), 2 * hh);
-          srcq[k2] = tile_off(r0 + ((inf >> 5) & 3), 2 * hh);
-          const T al = (kind == 0 || kind == 2) ? r.edge[k2].alen : (T)0;
-          anx[k2] = al * r.edge[k2].nx;
-          any[k2] = al * r.edge[k2].ny;
+        for (int w = tid; w < nh * NCH; w += NT) {
+          const int hs = w >> 2, cq = w & 3;
+          const ElemRec<T>& r = *reinterpret_cast<const ElemRec<T>*>(hrec + (size_t)hs * HR);
+          VecT qd[3], ud;
+          sweep_p1<T>(r, tl, 3 * (EB + hs), cq, vld<T>(vx + cq * W), vld<T>(vy + cq * W), dth, dth3, qd, ud);
         }
-        const int flags = r.flags;
+        __syncthreads();
+        // the other buffer's tile k - 1 is stored (or being stored): load tile k + 1
+        if (k + 1 < ntl) {
+          issue(vt0 + k + 1, bi ^ 1);
+          cp_async_commit();
+        }
+
+        // ---- phase 2: the update of block element j, half hh.  Row offsets
+        // are taken at chunk 2*hh; chunk 2*hh+1 of the same row is at offset ^ 16.
+        T rmt = (T)0, sqt = (T)0;
+        unsigned own[3];
 #pragma unroll
-        for (int cc = 0; cc < 2; ++cc) {
-          const int c = 2 * hh + cc;
-          const unsigned cx16 = 16u * cc;
-          const int vb = vb0 + c * W;
-          VecT(&out)[3] = outv[cc];
-          if (vb >= a.V) {  // all past V: the padding stays zero
+        for (int i = 0; i < 3; ++i) own[i] = tile_off(3 * j + i, 2 * hh);
+        VecT outv[2][3];
+        if (j < nb) {
+          const ElemRec<T>& r = recs[j];
+          const int e = e0 + j;
+          const T area3 = r.area * third;
+          T mudt[3], mmdt[3], cmx[3], cmn[3];
 #pragma unroll
-            for (int i = 0; i < 3; ++i) out[i] = VecT{};
-            continue;
-          }
-          const VecT cxv = vld<T>(vx + c * W), cyv = vld<T>(vy + c * W);
-          VecT g[3];
-#pragma unroll
-          for (int i = 0; i < 3; ++i) g[i] = vld<T>(tl + (own[i] ^ cx16));
-          // GETELC second half: RHS_i = AREA*(N_i,x FXME + N_i,y FYME), FXME
-          // = cx * mean(g), FYME = cy * mean(g); the P1 gradients sum to
-          // zero, so RHS_3 = -(RHS_1 + RHS_2)
-          T rhs[3][W];
-#pragma unroll
-          for (int w = 0; w < W; ++w) {
-            const T cx = VO::get(cxv, w), cy = VO::get(cyv, w);
-            const T s3 = (VO::get(g[0], w) + VO::get(g[1], w) + VO::get(g[2], w)) * area3;
-            rhs[0][w] = (r.gx[0] * cx + r.gy[0] * cy) * s3;
-            rhs[1][w] = (r.gx[1] * cx + r.gy[1] * cy) * s3;
-            rhs[2][w] = -(rhs[0][w] + rhs[1][w]);
-          }
-          // edge fluxes: RHS_p -= AL*SC*(2 u_p + u_q), RHS_q -= AL*SC*(u_p + 2 u_q)
-#pragma unroll
-          for (int k2 = 0; k2 < 3; ++k2) {
-            const int p = k2, qn = (k2 + 1) % 3;
-            const VecT gp = vld<T>(tl + (srcp[k2] ^ cx16)), gq = vld<T>(tl + (srcq[k2] ^ cx16));
-#pragma unroll
-            for (int w = 0; w < W; ++w) {
-              const T as = anx[k2] * VO::get(cxv, w) + any[k2] * VO::get(cyv, w);
-              const bool mine = as > (T)0;
-              const T up = mine ? VO::get(g[p], w) : VO::get(gp, w);
-              const T uq = mine ? VO::get(g[qn], w) : VO::get(gq, w);
-              rhs[p][w] -= as * ((T)2 * up + uq);
-              rhs[qn][w] -= as * (up + (T)2 * uq);
+          for (int i = 0; i < 3; ++i) {
+            mudt[i] = r.mu[i] * dt;
+            mmdt[i] = r.mm[i] * dt;
+            if (IMMAT == 0) {
+              cmx[i] = C.cmax[3 * e + i];
+              cmn[i] = C.cmin[3 * e + i];
             }
           }
-          if (flags & 0x38) {
-            // wall sides; molecules leaving the wall (src/getbou.f90:189-255)
-            // carry the fully diffuse part ALPHA*ETA*Mw (ALPHA < 1 is not built)
+          // per edge: the flux source's rows and AL*n (zero on inflow and
+          // wall sides, whose flux the wall path adds)
+          unsigned srcp[3], srcq[3];
+          T anx[3], any[3];
+#pragma unroll
+          for (int k2 = 0; k2 < 3; ++k2) {
+            const int inf = r.edge[k2].info, kind = inf & 3;
+            const int r0 = 3 * (inf >> 8);
+            srcp[k2] = tile_off(r0 + ((inf >> 3) & 3), 2 * hh);
+            srcq[k2] = tile_off(r0 + ((inf >> 5) & 3), 2 * hh);
+            const T al = (kind == 0 || kind == 2) ? r.edge[k2].alen : (T)0;
+            anx[k2] = al * r.edge[k2].nx;
+            any[k2] = al * r.edge[k2].ny;
+          }
+          const int flags = r.flags;
+#pragma unroll
+          for (int cc = 0; cc < 2; ++cc) {
+            const int cq = 2 * hh + cc;
+            const unsigned cx16 = 16u * cc;
+            const int vb = vb0 + cq * W;
+            VecT(&out)[3] = outv[cc];
+            if (vb >= C.V) {  // all past V: the padding stays zero
+#pragma unroll
+              for (int i = 0; i < 3; ++i) out[i] = VecT{};
+              continue;
+            }
+            const VecT cxv = vld<T>(vx + cq * W), cyv = vld<T>(vy + cq * W);
+            VecT g[3];
+#pragma unroll
+            for (int i = 0; i < 3; ++i) g[i] = vld<T>(tl + (own[i] ^ cx16));
+            // GETELC second half: RHS_i = AREA*(N_i,x FXME + N_i,y FYME), FXME
+            // = cx * mean(g), FYME = cy * mean(g); the P1 gradients sum to
+            // zero, so RHS_3 = -(RHS_1 + RHS_2)
+            T rhs[3][W];
+#pragma unroll
+            for (int w = 0; w < W; ++w) {
+              const T cx = VO::get(cxv, w), cy = VO::get(cyv, w);
+              const T s3 = (VO::get(g[0], w) + VO::get(g[1], w) + VO::get(g[2], w)) * area3;
+              rhs[0][w] = (r.gx[0] * cx + r.gy[0] * cy) * s3;
+              rhs[1][w] = (r.gx[1] * cx + r.gy[1] * cy) * s3;
+              rhs[2][w] = -(rhs[0][w] + rhs[1][w]);
+            }
+            // edge fluxes: RHS_p -= AL*SC*(2 u_p + u_q), RHS_q -= AL*SC*(u_p + 2 u_q)
 #pragma unroll
             for (int k2 = 0; k2 < 3; ++k2) {
-              if (!(flags & (8 << k2))) continue;
               const int p = k2, qn = (k2 + 1) % 3;
-              const int bs = r.bside[k2];
-              const T twr = (T)2 * a.rgas * a.bTw[bs];
-              const T uwx = a.bUw[2 * bs], uwy = a.bUw[2 * bs + 1], eta = a.bEta[bs];
-              const T nx = r.edge[k2].nx, ny = r.edge[k2].ny, alw = r.edge[k2].alen;
+              const VecT gp = vld<T>(tl + (srcp[k2] ^ cx16)), gq = vld<T>(tl + (srcq[k2] ^ cx16));
 #pragma unroll
               for (int w = 0; w < W; ++w) {
-                const T cx = VO::get(cxv, w), cy = VO::get(cyv, w);
-                const T sc = nx * cx + ny * cy;
-                T up, uq;
-                if (sc >= (T)0) {
-                  up = VO::get(g[p], w);
-                  uq = VO::get(g[qn], w);
-                } else {
-                  T mw;
-                  if (uwx == (T)0 && uwy == (T)0) {
-                    const T spd = sqrt(cx * cx + cy * cy);
-                    mw = dexp<T>(-(spd * spd) / twr);
-                  } else {
-                    const T dx = cx - uwx, dy = cy - uwy;
-                    mw = dexp<T>(-(dx * dx + dy * dy) / twr);
-                  }
-                  up = uq = a.alpha * (mw * eta);
-                }
-                const T as = alw * sc;
+                const T as = anx[k2] * VO::get(cxv, w) + any[k2] * VO::get(cyv, w);
+                const bool mine = as > (T)0;
+                const T up = mine ? VO::get(g[p], w) : VO::get(gp, w);
+                const T uq = mine ? VO::get(g[qn], w) : VO::get(gq, w);
                 rhs[p][w] -= as * ((T)2 * up + uq);
                 rhs[qn][w] -= as * (up + (T)2 * uq);
               }
             }
-          }
-          // GETINC / CMMINC, ADTHEM (f >= 0), INFLOW; the padding past V
-          // stays zero
-          auto finish = [&](auto full) {
+            if (flags & 0x38) {
+              // wall sides; molecules leaving the wall (src/getbou.f90:189-255)
+              // carry the fully diffuse part ALPHA*ETA*Mw (ALPHA < 1 is not built)
 #pragma unroll
-            for (int w = 0; w < W; ++w) {
-              const bool live = decltype(full)::value || vb + w < a.V;
-              const T u = VO::get(ur[cc], w);
+              for (int k2 = 0; k2 < 3; ++k2) {
+                if (!(flags & (8 << k2))) continue;
+                const int p = k2, qn = (k2 + 1) % 3;
+                const int bs = r.bside[k2];
+                const T twr = (T)2 * C.rgas * C.bTw[bs];
+                const T uwx = C.bUw[2 * bs], uwy = C.bUw[2 * bs + 1], eta = C.bEta[bs];
+                const T nx = r.edge[k2].nx, ny = r.edge[k2].ny, alw = r.edge[k2].alen;
 #pragma unroll
-              for (int i = 0; i < 3; ++i) {
-                const T f = VO::get(g[i], w) + u;
-                const T qmf = VO::get(qr[cc][i], w) - f;
-                T d, rr;
-                if (IMMAT == 1) {
-                  d = mmdt[i] * rhs[i][w] + mudt[i] * qmf;
-                  rr = fabs(d);
-                } else {
-                  const T x = rhs[i][w] * dt, cdt = mudt[i] * qmf;
-                  d = r.mm[i] * x + cdt;
-                  rr = ((x >= (T)0) ? cmx[i] : cmn[i]) * x + cdt;
-                  rr = rr > (T)0 ? rr : (T)0;
+                for (int w = 0; w < W; ++w) {
+                  const T cx = VO::get(cxv, w), cy = VO::get(cyv, w);
+                  const T sc = nx * cx + ny * cy;
+                  T up, uq;
+                  if (sc >= (T)0) {
+                    up = VO::get(g[p], w);
+                    uq = VO::get(g[qn], w);
+                  } else {
+                    T mw;
+                    if (uwx == (T)0 && uwy == (T)0) {
+                      const T spd = sqrt(cx * cx + cy * cy);
+                      mw = dexp<T>(-(spd * spd) / twr);
+                    } else {
+                      const T dx = cx - uwx, dy = cy - uwy;
+                      mw = dexp<T>(-(dx * dx + dy * dy) / twr);
+                    }
+                    up = uq = C.alpha * (mw * eta);
+                  }
+                  const T as = alw * sc;
+                  rhs[p][w] -= as * ((T)2 * up + uq);
+                  rhs[qn][w] -= as * (up + (T)2 * uq);
                 }
-                T fn = f + d;
-                // L2 residual: the change the unknown receives (-f where
-                // the clip applies; none at inflow-reset nodes)
-                const T ch = (fn < (T)0) ? -f : d;
-                fn = fn > (T)0 ? fn : (T)0;
-                if (live) {
-                  rmt = rr > rmt ? rr : rmt;
-                  if (!(flags & (1 << i))) sqt += ch * ch;
-                } else {
-                  fn = (T)0;
-                }
-                VO::set(out[i], w, fn);
               }
             }
-          };
-          if (vb + W <= a.V)
-            finish(std::true_type());
-          else
-            finish(std::false_type());
-          if (flags & 7) {
-            const VecT nf = vld<T>(vn + c * W);  // zero past V
+            // GETINC / CMMINC, ADTHEM (f >= 0), INFLOW; the padding past V
+            // stays zero
+            auto finish = [&](auto full) {
 #pragma unroll
-            for (int i = 0; i < 3; ++i)
-              if (flags & (1 << i)) out[i] = nf;
+              for (int w = 0; w < W; ++w) {
+                const bool live = decltype(full)::value || vb + w < C.V;
+                const T u = VO::get(ur[cc], w);
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                  const T f = VO::get(g[i], w) + u;
+                  const T qmf = VO::get(qr[cc][i], w) - f;
+                  T d, rr;
+                  if (IMMAT == 1) {
+                    d = mmdt[i] * rhs[i][w] + mudt[i] * qmf;
+                    rr = fabs(d);
+                  } else {
+                    const T x = rhs[i][w] * dt, cdt = mudt[i] * qmf;
+                    d = r.mm[i] * x + cdt;
+                    rr = ((x >= (T)0) ? cmx[i] : cmn[i]) * x + cdt;
+                    rr = rr > (T)0 ? rr : (T)0;
+                  }
+                  T fn = f + d;
+                  // L2 residual: the change the unknown receives (-f where
+                  // the clip applies; none at inflow-reset nodes)
+                  const T ch = (fn < (T)0) ? -f : d;
+                  fn = fn > (T)0 ? fn : (T)0;
+                  if (live) {
+                    rmt = rr > rmt ? rr : rmt;
+                    if (!(flags & (1 << i))) sqt += ch * ch;
+                  } else {
+                    fn = (T)0;
+                  }
+                  VO::set(out[i], w, fn);
+                }
+              }
+            };
+            if (vb + W <= C.V)
+              finish(std::true_type());
+            else
+              finish(std::false_type());
+            if (flags & 7) {
+              const VecT nf = vld<T>(vn + cq * W);  // zero past V
+#pragma unroll
+              for (int i = 0; i < 3; ++i)
+                if (flags & (1 << i)) out[i] = nf;
+            }
           }
         }
-      }
-      rmax = fmax(rmax, (double)rmt);
-      rsq += (double)sqt;
-      // every thread is past its phase-2 reads of tile k: the new rows
-      // replace the block rows in the buffer, for the box store
-      __syncthreads();
-      if (j < nb) {
+        rmax = fmax(rmax, (double)rmt);
+        rsq += (double)sqt;
+        // every thread is past its phase-2 reads of tile k: the new rows
+        // replace the block rows in the buffer, for the box store
+        __syncthreads();
+        if (j < nb) {
 #pragma unroll
-        for (int cc = 0; cc < 2; ++cc)
+          for (int cc = 0; cc < 2; ++cc)
 #pragma unroll
-          for (int i = 0; i < 3; ++i) vst<T>(tl + (own[i] ^ (16u * cc)), outv[cc][i]);
+            for (int i = 0; i < 3; ++i) vst<T>(tl + (own[i] ^ (16u * cc)), outv[cc][i]);
+        }
+        fence_proxy_async_smem();
       }
-      fence_proxy_async_smem();
-    }
-    if (aborted) {
-      // a bounded wait expired (the vote made every thread leave the tile
-      // loop together): drain this CTA's box copies in flight, bounded, and
-      // report through the control block
-      if (tid == 0) {
-        a.ctrl->timeout = 1;
-        mbar_wait_bounded(&bars[abort_buf], ((par >> abort_buf) & 1u) ^ 1u);
-        bulk_wait0();
+      if (aborted) {
+        // a bounded wait expired (the vote made every thread leave the tile
+        // loop together): drain this CTA's copies in flight, bounded, and
+        // report through the case's control block
+        if (tid == 0) {
+          C.ctrl->timeout = 1;
+          mbar_wait_bounded(&bars[abort_buf], ((par >> abort_buf) & 1u) ^ 1u);
+          bulk_wait0();
+        }
+        return;
       }
-      return;
+      // the unit's residual, per warp
+      rmax = warp_max(rmax);
+      rsq = warp_sum(rsq);
+      if ((tid & 31) == 0) {
+        red_m[tid >> 5] = rmax;
+        red_s[tid >> 5] = rsq;
+      }
+      last_map = &C.tm[cur ^ 1];
+      last_vt = vt0 + ntl - 1;
+      last_bi = (ntl - 1) & 1;
+      last_y0 = 3 * e0;
     }
     // every thread is past phase 2 of the unit's last tile and has written
-    // its rows: store the last tile; the records, tables and halo list may
+    // its rows: store the last tile and add the unit's residual to its case
+    // (the sum of squares can differ in its last bits between runs: the
+    // order of the atomics varies); the records, tables and halo list may
     // be replaced
     if (tid == 0) s_unit = next;
     __syncthreads();
-    if (tid == 0) store(vt0 + ntl - 1, (ntl - 1) & 1);
-    unit = s_unit;
-    if (tid == 0 && unit < nunits) next = (int)gridDim.x + atomicAdd(&a.ctrl->sweep_next, 1);
-  }
-  // per-CTA residual partials, reduced by k_resid (the sum of squares can
-  // differ in its last bits between runs: which units a CTA draws varies)
-  rmax = warp_max(rmax);
-  rsq = warp_sum(rsq);
-  if ((tid & 31) == 0) {
-    red_m[tid >> 5] = rmax;
-    red_s[tid >> 5] = rsq;
-  }
-  __syncthreads();
-  if (tid == 0) {
-    double mm = 0, ss = 0;
-    for (int w = 0; w < NW; ++w) {
-      mm = fmax(mm, red_m[w]);
-      ss += red_s[w];
+    if (tid == 0 && last_map) {
+      store(last_map, last_vt, last_bi, last_y0);
+      double mm = 0, ss = 0;
+      for (int w = 0; w < NW; ++w) {
+        mm = fmax(mm, red_m[w]);
+        ss += red_s[w];
+      }
+      atomicAdd(&C.ctrl->acc_sq, ss);
+      atomicMax(reinterpret_cast<unsigned long long*>(&C.ctrl->acc_max), (unsigned long long)__double_as_longlong(mm));
     }
-    a.part_max[blockIdx.x] = mm;
-    a.part_sq[blockIdx.x] = ss;
-    bulk_wait0();  // the last box stores are complete before the CTA exits
+    unit = s_unit;
+    if (tid == 0 && unit < total_units) next = (int)gridDim.x + atomicAdd(&a.ctl->sweep_next, 1);
   }
+  if (tid == 0) bulk_wait0();  // the last box stores are complete before the CTA exits
 }
 
 // ----------------------------------------------------------- residual ----
-struct ResidArgs {
-  const double* part_max;
-  const double* part_sq;
-  double* hist_linf;
-  double* hist_l2;
-  double* hist_dt;
-  Ctrl* ctrl;
-};
-
-__global__ void __launch_bounds__(1024) k_resid(ResidArgs a) {
-  Ctrl* c = a.ctrl;
+// GETRES + the residual bookkeeping (src/advnce.f90:385, 422-429) per case,
+// one thread per case: the step's max and L2 residual into the history, the
+// non-finite and convergence tests, the step counter and the buffer swap;
+// the step's accumulators are cleared for the next step.
+template <class T> __global__ void k_resid(BatchArgs<T> a) {
+  if (threadIdx.x != 0) return;
+  if (blockIdx.x == 0) a.ctl->sweep_next = 0;
+  const CaseDev<T>& C = a.cases[blockIdx.x];
+  Ctrl* c = C.ctrl;
   if (c->done) return;
-  __shared__ double sm[32], ss[32];
-  double m = 0, s = 0;
-  for (int i = threadIdx.x; i < c->nparts; i += blockDim.x) {
-    m = fmax(m, a.part_max[i]);
-    s += a.part_sq[i];
+  const double mm = c->acc_max, sq = c->acc_sq;
+  const int st = c->step;
+  const double l2 = sqrt(sq);
+  C.hist_linf[st] = mm;
+  C.hist_l2[st] = l2;
+  C.hist_dt[st] = step_dt(c);
+  if (!isfinite(l2) || !isfinite(mm)) {
+    c->nonfinite = 1;
+    c->done = 1;
   }
-  int bad = (isnan(m) || isnan(s)) ? 1 : 0;
-  bad = __syncthreads_or(bad);
-  m = warp_max(m);
-  s = warp_sum(s);
-  if ((threadIdx.x & 31) == 0) {
-    sm[threadIdx.x >> 5] = m;
-    ss[threadIdx.x >> 5] = s;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double mm = 0, sq = 0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
-      mm = fmax(mm, sm[w]);
-      sq += ss[w];
-    }
-    const int st = c->step;
-    const double l2 = sqrt(sq);
-    a.hist_linf[st] = mm;
-    a.hist_l2[st] = l2;
-    a.hist_dt[st] = step_dt(c);
-    if (bad || !isfinite(l2) || !isfinite(mm)) {
-      c->nonfinite = 1;
-      c->done = 1;
-    }
-    if (c->timeout) c->done = 1;
-    if (c->ref == 0.0 && l2 > 0.0) c->ref = l2;
-    c->sweep_next = 0;
-    c->step = st + 1;
-    if (c->step >= c->max_steps) c->done = 1;
-    if (c->tol > 0.0 && l2 <= c->tol * c->ref) c->done = 1;
-  }
+  if (c->timeout) c->done = 1;
+  if (c->ref == 0.0 && l2 > 0.0) c->ref = l2;
+  c->acc_sq = 0.0;
+  c->acc_max = 0.0;
+  c->maxmu = 0.0;
+  c->cur ^= 1;
+  c->step = st + 1;
+  if (c->step >= c->max_steps) c->done = 1;
+  if (c->tol > 0.0 && l2 <= c->tol * c->ref) c->done = 1;
 }
 
 // -------------------------------------------------------------- nodal ----

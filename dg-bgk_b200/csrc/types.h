@@ -64,19 +64,26 @@ struct WallSide {
   double sumbottom;    // sqrt(2*PI*R^3*T_w^3)
 };
 
-// Device-side control block of one handle.
+// Device-side control block of one case.
 struct Ctrl {
-  int done;       // kernels return at once when set
+  int done;       // kernels skip the case when set
   int step;       // steps run in this advance call
   int max_steps;
   int nonfinite;  // set when a residual was NaN/Inf
   double tol;     // relative L2 tolerance (<= 0: none)
   double ref;     // reference L2 residual (0: take the first step's)
-  double maxmu;   // max MU of the current step (atomicMax on the bits)
+  double maxmu;   // max MU of the current step (atomicMax on the bits; reset by k_resid)
   double dtc;     // Courant limit DTEc (src/alotim.f90)
-  int nparts;     // sweep CTAs writing residual partials
+  double acc_sq;  // sum of squared changes of the current step (sweep atomics; reset by k_resid)
+  double acc_max; // max residual of the current step (atomicMax on the bits; reset by k_resid)
+  int cur;        // which f buffer holds the current state (k_resid swaps it)
   int timeout;    // set when a bounded device wait gave up
-  int sweep_next; // sweep work units handed out beyond the first wave (reset by k_resid)
+};
+
+// Device-side control of one launch set (a case alone or a batch).
+struct BatchCtl {
+  int sweep_next;  // sweep work units handed out beyond the first wave (reset by k_resid)
+  int pad[15];
 };
 
 }  // namespace dgbgk

@@ -51,6 +51,10 @@ class Params(ctypes.Structure):
     ]
 
 
+class BatchParams(ctypes.Structure):
+    _fields_ = [("tile_elems", c_int), ("units_per_cta", c_int), ("tune_steps", c_int)]
+
+
 # name -> (restype, argtypes); mirrors include/dgbgk.h
 _PD = POINTER(c_double)
 _PI = POINTER(c_int)
@@ -78,6 +82,13 @@ SIGNATURES = {
     "dgbgk_profile_steps": (c_int, [c_void_p, c_int, _PD]),
     "dgbgk_destroy": (None, [c_void_p]),
     "dgbgk_last_error": (ctypes.c_char_p, []),
+    "dgbgk_batch_default_params": (None, [POINTER(BatchParams)]),
+    "dgbgk_batch_create": (c_int, [POINTER(c_void_p), c_int, POINTER(BatchParams), POINTER(c_void_p)]),
+    "dgbgk_batch_advance": (c_int, [c_void_p, c_int, c_double, _PI, _PD]),
+    "dgbgk_batch_info": (c_int, [c_void_p, _PI]),
+    "dgbgk_batch_tuning": (c_int, [c_void_p, c_int, _PD]),
+    "dgbgk_batch_last_timing": (c_int, [c_void_p, _PD]),
+    "dgbgk_batch_destroy": (None, [c_void_p]),
 }
 
 _lib = None

@@ -228,6 +228,23 @@ def config5():
     return channel_case(-10.0, 30.0, -10.0, 10.0, 400, 200, 32, 64, mach=1.5, kn=0.02)
 
 
+def config3(ncases=64, seed=1, n_choices=tuple(range(16, 97, 8))):
+    """The batched workload: `ncases` lid-driven cavities, each with its own
+    draw (numpy PCG64, `seed`) of the mesh size N from `n_choices`, radial
+    velocities from 8..24, angles from 16..64, lid Mach from U[0.1, 1] and
+    Kn from logU[0.01, 1]; case k's density perturbation uses seed 1000 + k."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for k in range(ncases):
+        n = int(rng.choice(n_choices))
+        nr = int(rng.integers(8, 25))
+        nt = int(rng.integers(16, 65))
+        mach = float(rng.uniform(0.1, 1.0))
+        kn = float(10.0 ** rng.uniform(-2.0, 0.0))
+        out.append(cavity_case(n, nr, nt, mach=mach, kn=kn, seed=1000 + k))
+    return out
+
+
 def node_scale(case):
     """Per-DG-node density factor (3,NELEM) of the seeded perturbation, or
     None without one."""

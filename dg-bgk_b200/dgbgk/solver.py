@@ -231,3 +231,60 @@ class Solver:
         keys = ["nelem", "npoin", "nboun", "nside", "vnpnt", "precision", "tile_elems", "tile_vels", "n_blocks",
                 "max_halo"]
         return dict(zip(keys, (int(x) for x in o)))
+
+
+class Batch:
+    """Many Solver cases advanced together (dgbgk_batch_*): one persistent
+    launch per kernel and step over all the cases, steps replayed from one
+    CUDA graph, tile shape chosen by the library's autotuner.  The solvers
+    must share precision, IMMAT and device; they stay usable on their own
+    between batch calls."""
+
+    TUNE_KEYS = [(eb, upc) for eb in (64, 128) for upc in (2, 4, 8, 16)] + [("rows", r) for r in (1, 2, 4)]
+
+    def __init__(self, solvers, tile_elems=0, units_per_cta=0, tune_steps=4):
+        from ._lib import BatchParams
+        self.solvers = list(solvers)
+        p = BatchParams()
+        lib().dgbgk_batch_default_params(ctypes.byref(p))
+        p.tile_elems = tile_elems
+        p.units_per_cta = units_per_cta
+        p.tune_steps = tune_steps
+        hs = (c_void_p * len(self.solvers))(*[s.h for s in self.solvers])
+        b = c_void_p()
+        check(lib().dgbgk_batch_create(hs, len(self.solvers), ctypes.byref(p), ctypes.byref(b)))
+        self.h = b
+
+    def advance(self, max_steps, tol=0.0):
+        n = len(self.solvers)
+        steps = np.zeros(n, dtype=np.int32)
+        l2 = np.zeros(n)
+        check(lib().dgbgk_batch_advance(self.h, max_steps, tol, ptr(steps, c_int), ptr(l2)))
+        return {"steps": steps, "res_l2_last": l2}
+
+    def info(self):
+        o = np.zeros(7, dtype=np.int32)
+        check(lib().dgbgk_batch_info(self.h, ptr(o, c_int)))
+        return dict(zip(["ncases", "tile_elems", "units_per_cta", "sweep_units", "sweep_ctas", "moment_ctas",
+                         "moment_rows"], (int(x) for x in o)))
+
+    def tuning(self):
+        ms = np.zeros(11)
+        check(lib().dgbgk_batch_tuning(self.h, 11, ptr(ms)))
+        return {k: float(v) for k, v in zip(self.TUNE_KEYS, ms) if v > 0}
+
+    def last_ms(self):
+        t = c_double(0)
+        check(lib().dgbgk_batch_last_timing(self.h, ctypes.byref(t)))
+        return t.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().dgbgk_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -138,8 +138,9 @@ int dgbgk_init_maxwellian(dgbgk_handle* h, const double* n, const double* u, con
  * residual of the first step this handle ever ran unless set with
  * dgbgk_set_residual_reference().  Per step, when non-NULL, res_linf gets
  * max|DELUN| (the value behind RESIDUAL.RES, src/advnce.f90:422-429),
- * res_l2 the L2 norm of DELUN and dte the time step.  *steps_done gets the
- * number of steps run. */
+ * res_l2 the L2 norm of the change the unknowns receive (DELUN, -f where
+ * ADTHEM clips, nothing at the DG nodes INFLOW resets) and dte the time
+ * step.  *steps_done gets the number of steps run. */
 int dgbgk_advance(dgbgk_handle* h, int max_steps, double tol_rel, int* steps_done, double* res_linf,
                   double* res_l2, double* dte);
 int dgbgk_set_residual_reference(dgbgk_handle* h, double res_l2_ref);
@@ -192,6 +193,53 @@ int dgbgk_get_macros_noalloc(dgbgk_handle* h, double* nd, double* rho, double* u
 
 void dgbgk_destroy(dgbgk_handle* h);
 const char* dgbgk_last_error(void);
+
+/* ---- Batches (no counterpart in the reference) --------------------------
+ * Many cases -- handles of the same precision, IMMAT and device, each with
+ * its own mesh, velocity grid and state -- advanced together: every kernel
+ * of a pseudo-time step is one persistent launch over the flattened work of
+ * all the cases, and steps are replayed from one CUDA graph.  Each case
+ * keeps its own time step, residual history, reference and convergence
+ * test; cases that converge (or reach max_steps) stop while the others go
+ * on.  The handles stay usable on their own between batch calls (not
+ * concurrently with them). */
+typedef struct dgbgk_batch dgbgk_batch;
+
+typedef struct {
+  int tile_elems;     /* sweep elements per CTA, 64 or 128 (0: autotuned)    */
+  int units_per_cta;  /* sweep work units per resident CTA, 2/4/8/16 (0: autotuned) */
+  int tune_steps;     /* steps timed per autotuner candidate                */
+} dgbgk_batch_params;
+
+void dgbgk_batch_default_params(dgbgk_batch_params* p);
+
+/* Creates a batch over `ncases` handles.  The autotuner times every
+ * candidate tile shape (elements per CTA x units per CTA) on the cases'
+ * current states for `tune_steps` steps, restores the states, and keeps
+ * the fastest. */
+int dgbgk_batch_create(dgbgk_handle* const* cases, int ncases, const dgbgk_batch_params* p,
+                       dgbgk_batch** out);
+
+/* Advances every case until its L2 residual falls to tol times its
+ * reference (tol <= 0: no test) or it has run max_steps steps.
+ * steps_done[ncases] and res_l2_last[ncases] (either may be NULL) receive
+ * each case's step count and last L2 residual; the per-step histories stay
+ * in the handles' devices and are not returned here. */
+int dgbgk_batch_advance(dgbgk_batch* b, int max_steps, double tol, int* steps_done, double* res_l2_last);
+
+/* [ncases, tile_elems, units_per_cta, sweep work units, sweep CTAs,
+ * moment CTAs, moment rows per warp step] of the chosen configuration. */
+int dgbgk_batch_info(const dgbgk_batch* b, int* out7);
+
+/* The autotuner's ms per batch step: (tile_elems 64, 128) x (units_per_cta
+ * 2, 4, 8, 16), then moment rows per warp step 1, 2, 4 at the chosen sweep
+ * shape; 0 where not tried; n <= 11. */
+int dgbgk_batch_tuning(const dgbgk_batch* b, int n, double* ms_per_step);
+
+/* Device time of the last dgbgk_batch_advance() in ms. */
+int dgbgk_batch_last_timing(const dgbgk_batch* b, double* total_ms);
+
+void dgbgk_batch_destroy(dgbgk_batch* b);
 
 #ifdef __cplusplus
 }

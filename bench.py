@@ -45,6 +45,7 @@ def args():
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain-FP64 comparison leg")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-steady", action="store_true", help="skip the time-to-steady-state leg")
     return ap.parse_args()
 
 
@@ -265,6 +266,31 @@ def run_ours(a, d):
                        "kernel_ms": dict(zip(names, [float(x) for x in k64]))}
         out["fp32_over_fp64_per_step"] = out["value"] / out["fp64"]["value"]
         del s64
+    # time to steady state (L2 residual 1e-8 of the first step's), cold
+    # start, plain FP64 vs FP32, on a 16^2 lid-driven cavity (16x32
+    # velocities), small enough to converge within the bench
+    if not a.no_steady:
+        from dgbgk import cavity_case
+        from dgbgk.steady import cold_march
+        sc = cavity_case(16, 16, 32, mach=0.3, kn=0.1)
+        st = {"case": sc.name, "dofs": sc.dofs, "tol": 1e-8, "start": "cold (rest Maxwellian, seeded 1e-3 "
+              "density perturbation)"}
+        for prec in (64, 32):
+            r, so = cold_march(sc, prec, 1e-8, 3000000, device=d.local)
+            r["device_s"] = d.max(r["device_s"])
+            st[f"fp{prec}"] = {k: r[k] for k in ("steps", "device_s", "res_rel", "converged")}
+            if prec == 64:
+                m64 = so.macros()
+            else:
+                m32 = so.macros()
+            del so
+        st["fp32_speedup"] = st["fp64"]["device_s"] / st["fp32"]["device_s"]
+        st["fp32_vs_fp64_rel_l2"] = {k: float(np.linalg.norm(m32[k] - m64[k]) / max(np.linalg.norm(m64[k]), 1e-300))
+                                     for k in ("rho", "temp")}
+        vs = float(np.sqrt(sc.rgas * sc.init["T1"]))  # velocities on the thermal-speed scale
+        for k in ("u", "v"):
+            st["fp32_vs_fp64_rel_l2"][k] = float(np.linalg.norm(m32[k] - m64[k]) / (vs * np.sqrt(len(m64[k]))))
+        out["steady_state"] = st
     # end to end through the C ABI with host buffers
     if not a.no_e2e:
         s = Solver.from_case(case, precision=a.precision, device=d.local)

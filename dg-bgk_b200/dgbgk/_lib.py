@@ -89,6 +89,15 @@ SIGNATURES = {
     "dgbgk_batch_tuning": (c_int, [c_void_p, c_int, _PD]),
     "dgbgk_batch_last_timing": (c_int, [c_void_p, _PD]),
     "dgbgk_batch_destroy": (None, [c_void_p]),
+    "dgbgk_mlp_create": (c_int, [c_int, c_int, c_int, c_int, c_int, ctypes.c_ulonglong, c_int, POINTER(c_void_p)]),
+    "dgbgk_mlp_param_count": (ctypes.c_longlong, [c_void_p]),
+    "dgbgk_mlp_get_params": (c_int, [c_void_p, POINTER(c_float)]),
+    "dgbgk_mlp_set_params": (c_int, [c_void_p, POINTER(c_float)]),
+    "dgbgk_mlp_forward": (c_int, [c_void_p, POINTER(c_float), c_int, POINTER(c_float)]),
+    "dgbgk_mlp_gradient": (c_int, [c_void_p, POINTER(c_float), POINTER(c_float), c_int, _PD, POINTER(c_float)]),
+    "dgbgk_mlp_set_data": (c_int, [c_void_p, POINTER(c_float), POINTER(c_float), c_int]),
+    "dgbgk_mlp_train": (c_int, [c_void_p, c_int, c_float, ctypes.c_ulonglong, _PD]),
+    "dgbgk_mlp_destroy": (None, [c_void_p]),
 }
 
 _lib = None

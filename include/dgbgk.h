@@ -241,6 +241,34 @@ int dgbgk_batch_last_timing(const dgbgk_batch* b, double* total_ms);
 
 void dgbgk_batch_destroy(dgbgk_batch* b);
 
+/* ---- Warm-start network (no counterpart in the reference) ---------------
+ * A multilayer perceptron n_in -> width x depth (tanh) -> n_out trained and
+ * evaluated with hand-written BF16 tensor-core kernels (tcgen05, FP32
+ * accumulation in tensor memory, FP32 master weights, Adam).  It maps case
+ * parameters to resampled steady fields whose Maxwellian starts the solver
+ * (dgbgk_init_maxwellian).  Sizes: n_in <= 64; width, n_out and batch
+ * multiples of 128. */
+typedef struct dgbgk_mlp dgbgk_mlp;
+
+int dgbgk_mlp_create(int n_in, int width, int depth, int n_out, int batch, unsigned long long seed, int device,
+                     dgbgk_mlp** out);
+/* Number of parameters; per layer W[out][in] (the input layer's in is 64,
+ * columns past n_in zero) then b[out], layers in order. */
+long long dgbgk_mlp_param_count(const dgbgk_mlp* m);
+int dgbgk_mlp_get_params(dgbgk_mlp* m, float* params);
+int dgbgk_mlp_set_params(dgbgk_mlp* m, const float* params);
+/* y[n][n_out] = network(x[n][n_in]) */
+int dgbgk_mlp_forward(dgbgk_mlp* m, const float* x, int n, float* y);
+/* Mean squared error and its gradient (the parameter layout) on one batch
+ * of exactly `batch` rows. */
+int dgbgk_mlp_gradient(dgbgk_mlp* m, const float* x, const float* t, int n, double* loss, float* grad);
+/* Training set x[n][n_in], t[n][n_out], kept on the device. */
+int dgbgk_mlp_set_data(dgbgk_mlp* m, const float* x, const float* t, int n);
+/* iters Adam steps (learning rate lr) on minibatches drawn without
+ * replacement per epoch (seeded); loss_hist[iters] may be NULL. */
+int dgbgk_mlp_train(dgbgk_mlp* m, int iters, float lr, unsigned long long seed, double* loss_hist);
+void dgbgk_mlp_destroy(dgbgk_mlp* m);
+
 #ifdef __cplusplus
 }
 #endif

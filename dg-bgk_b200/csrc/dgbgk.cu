@@ -83,6 +83,10 @@ struct ImplBase {
   virtual int profile(int nsteps, double* ms) = 0;
   virtual int macros_noalloc(double* scratch, double* nd, double* rho, double* u, double* v, double* ps,
                              double* temp) = 0;
+  // the state in the reference layout DISNF(3,VNPNT,NELEM), FP64, from / to
+  // a device buffer (the stream is synchronised on return)
+  virtual int export_device(double* buf) = 0;
+  virtual int import_device(const double* buf) = 0;
   Plan pl;
   int device = 0;
   int prec = 64;
@@ -725,6 +729,23 @@ template <class T> struct Impl : ImplBase {
     CK(cudaStreamSynchronize(st));
     return 0;
   }
+  int export_device(double* buf) override {
+    CK(cudaSetDevice(device));
+    TRY(upload_perm());
+    k_from_internal<T, double><<<pl.E, 256, 0, st>>>(f[cur], buf, d_inv, pl.V, Vp);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(st));
+    return 0;
+  }
+  int import_device(const double* buf) override {
+    CK(cudaSetDevice(device));
+    TRY(upload_perm());
+    k_to_internal<double, T><<<pl.E, 256, 0, st>>>(buf, f[0], d_inv, pl.V, Vp);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(st));
+    cur = 0;
+    return 0;
+  }
   int upload_perm() {
     if (d_inv) return 0;
     TRY(upload(&d_inv, pl.inv, st));
@@ -1030,6 +1051,24 @@ int dgbgk_get_residual_reference(dgbgk_handle* h, double* r) {
   *r = h->impl->ref_host;
   return 0;
 }
+int dgbgk_copy_state(dgbgk_handle* dst, const dgbgk_handle* src) {
+  HCHECK(dst);
+  HCHECK(src);
+  ImplBase* d = dst->impl.get();
+  ImplBase* s_ = src->impl.get();
+  if (d->device != s_->device || d->pl.E != s_->pl.E || d->pl.V != s_->pl.V || d->pl.NP != s_->pl.NP ||
+      d->pl.B != s_->pl.B)
+    return set_error("dgbgk_copy_state: the handles differ in device, mesh or velocity grid"), DGBGK_EINVAL;
+  if (d == s_) return 0;
+  CK(cudaSetDevice(d->device));
+  double* buf = nullptr;
+  CK(cudaMalloc(&buf, (size_t)3 * d->pl.E * d->pl.V * sizeof(double)));
+  int rc = s_->export_device(buf);
+  if (rc == 0) rc = d->import_device(buf);
+  cudaFree(buf);
+  if (rc == 0) d->ref_host = s_->ref_host;
+  return rc;
+}
 int dgbgk_get_macros(dgbgk_handle* h, double* nd, double* rho, double* u, double* v, double* ps, double* temp) {
   HCHECK(h);
   return h->impl->macros(nd, rho, u, v, ps, temp);
@@ -1084,6 +1123,7 @@ struct BatchBase {
   virtual void info(int* out) const = 0;
   virtual int tuning(int n, double* ms) const = 0;
   float last_ms = 0.f;
+  std::vector<int> last_rc;  // per case: the status of the last advance
 };
 
 template <class T> struct BatchImpl : BatchBase {
@@ -1315,11 +1355,13 @@ template <class T> struct BatchImpl : BatchBase {
     CK(cudaStreamSynchronize(st));
     CK(cudaEventElapsedTime(&last_ms, ev0, ev1));
     int rc = 0;
+    last_rc.assign(cs.size(), 0);
     for (size_t i = 0; i < cs.size(); ++i) {
       Impl<T>* c = cs[i];
       CK(cudaMemcpy(&c->hctrl[1], c->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost));
       int ns = 0;
       const int r = c->collect(c->hctrl[1], &ns, nullptr, nullptr, nullptr);
+      last_rc[i] = r;
       if (r != 0 && rc == 0) rc = r;
       if (steps) steps[i] = ns;
       if (l2) {
@@ -1407,6 +1449,12 @@ int dgbgk_batch_create(dgbgk_handle* const* cases, int ncases, const dgbgk_batch
 int dgbgk_batch_advance(dgbgk_batch* b, int max_steps, double tol, int* steps_done, double* res_l2_last) {
   if (!b || !b->impl) return set_error("NULL batch"), DGBGK_EINVAL;
   return b->impl->advance(max_steps, tol, steps_done, res_l2_last);
+}
+
+int dgbgk_batch_status(const dgbgk_batch* b, int* status) {
+  if (!b || !b->impl || !status) return set_error("NULL batch"), DGBGK_EINVAL;
+  for (size_t i = 0; i < b->impl->last_rc.size(); ++i) status[i] = b->impl->last_rc[i];
+  return DGBGK_OK;
 }
 
 int dgbgk_batch_info(const dgbgk_batch* b, int* out) {

@@ -73,6 +73,7 @@ SIGNATURES = {
     "dgbgk_advance": (c_int, [c_void_p, c_int, c_double, _PI, _PD, _PD, _PD]),
     "dgbgk_set_residual_reference": (c_int, [c_void_p, c_double]),
     "dgbgk_get_residual_reference": (c_int, [c_void_p, _PD]),
+    "dgbgk_copy_state": (c_int, [c_void_p, c_void_p]),
     "dgbgk_get_macros": (c_int, [c_void_p, _PD, _PD, _PD, _PD, _PD, _PD]),
     "dgbgk_get_macros_noalloc": (c_int, [c_void_p, _PD, _PD, _PD, _PD, _PD, _PD]),
     "dgbgk_get_node_fields": (c_int, [c_void_p, _PD, _PD, _PD, _PD, _PD]),
@@ -85,6 +86,7 @@ SIGNATURES = {
     "dgbgk_batch_default_params": (None, [POINTER(BatchParams)]),
     "dgbgk_batch_create": (c_int, [POINTER(c_void_p), c_int, POINTER(BatchParams), POINTER(c_void_p)]),
     "dgbgk_batch_advance": (c_int, [c_void_p, c_int, c_double, _PI, _PD]),
+    "dgbgk_batch_status": (c_int, [c_void_p, _PI]),
     "dgbgk_batch_info": (c_int, [c_void_p, _PI]),
     "dgbgk_batch_tuning": (c_int, [c_void_p, c_int, _PD]),
     "dgbgk_batch_last_timing": (c_int, [c_void_p, _PD]),

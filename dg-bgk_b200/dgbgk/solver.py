@@ -209,6 +209,11 @@ class Solver:
         check(lib().dgbgk_get_residual_reference(self.h, ctypes.byref(r)))
         return r.value
 
+    def copy_state_from(self, other):
+        """Takes `other`'s state (converted to this handle's precision on the
+        device) and residual reference; same mesh and velocity grid."""
+        check(lib().dgbgk_copy_state(self.h, other.h))
+
     # -- observables ----------------------------------------------------
     def macros(self):
         out = {k: np.zeros(self.NP) for k in ("nd", "rho", "u", "v", "ps", "temp")}
@@ -255,12 +260,20 @@ class Batch:
         check(lib().dgbgk_batch_create(hs, len(self.solvers), ctypes.byref(p), ctypes.byref(b)))
         self.h = b
 
-    def advance(self, max_steps, tol=0.0):
+    def advance(self, max_steps, tol=0.0, raise_on_error=True):
+        """Steps every case to tol (relative to its reference) or max_steps.
+        With raise_on_error=False a case that diverges only stops: its
+        status (0, or the error code) is in the result."""
         n = len(self.solvers)
         steps = np.zeros(n, dtype=np.int32)
         l2 = np.zeros(n)
-        check(lib().dgbgk_batch_advance(self.h, max_steps, tol, ptr(steps, c_int), ptr(l2)))
-        return {"steps": steps, "res_l2_last": l2}
+        rc = lib().dgbgk_batch_advance(self.h, max_steps, tol, ptr(steps, c_int), ptr(l2))
+        status = np.zeros(n, dtype=np.int32)
+        check(lib().dgbgk_batch_status(self.h, ptr(status, c_int)))
+        diverged_only = bool(np.isin(status, (0, _lib.DGBGK_ENONFINITE)).all() and (status != 0).any())
+        if rc != 0 and (raise_on_error or not diverged_only):
+            check(rc)
+        return {"steps": steps, "res_l2_last": l2, "status": status}
 
     def info(self):
         o = np.zeros(7, dtype=np.int32)

@@ -146,6 +146,13 @@ int dgbgk_advance(dgbgk_handle* h, int max_steps, double tol_rel, int* steps_don
 int dgbgk_set_residual_reference(dgbgk_handle* h, double res_l2_ref);
 int dgbgk_get_residual_reference(dgbgk_handle* h, double* res_l2_ref);
 
+/* No counterpart in the reference.  Copies the state of `src` into `dst`
+ * on the device, converting between the handles' precisions (FP32 <-> FP64),
+ * and hands over the residual reference: the precision handoff of a march
+ * that runs its transient in FP32 and finishes in FP64.  Both handles must
+ * be on one device and built from the same mesh and velocity grid. */
+int dgbgk_copy_state(dgbgk_handle* dst, const dgbgk_handle* src);
+
 /* MACROS (src/macros.f90:51-188) + GETMAC (src/getmac.f90:98-123) of the
  * current state: nodal ND, RHO, UVEL, VVEL, PS, TEMP, NPOIN values each. */
 int dgbgk_get_macros(dgbgk_handle* h, double* nd, double* rho, double* u, double* v, double* ps,
@@ -226,6 +233,11 @@ int dgbgk_batch_create(dgbgk_handle* const* cases, int ncases, const dgbgk_batch
  * each case's step count and last L2 residual; the per-step histories stay
  * in the handles' devices and are not returned here. */
 int dgbgk_batch_advance(dgbgk_batch* b, int max_steps, double tol, int* steps_done, double* res_l2_last);
+
+/* status[ncases]: each case's result of the last dgbgk_batch_advance()
+ * (DGBGK_OK, DGBGK_ENONFINITE for a case that diverged and stopped, ...);
+ * the advance itself returns the first non-zero one. */
+int dgbgk_batch_status(const dgbgk_batch* b, int* status);
 
 /* [ncases, tile_elems, units_per_cta, sweep work units, sweep CTAs,
  * moment CTAs, moment rows per warp step] of the chosen configuration. */

@@ -130,11 +130,19 @@ def cavity_mesh(n, lid_speed=0.0):
     return RawMesh(intma, coord, bsido, wv, {"kind": "cavity", "n": n, "lid_speed": lid_speed})
 
 
-def channel_mesh(x0, x1, y0, y1, nx, ny, obstacle_side=1.0, center=(0.0, 0.0)):
+def channel_mesh(x0, x1, y0, y1, nx, ny, obstacle_side=1.0, center=(0.0, 0.0), sides="outflow"):
     """Channel [x0,x1]x[y0,y1] of nx x ny quads; quads whose centres lie in
     the square obstacle (side obstacle_side, snapped to whole cells) are
-    removed.  Left: inflow (type 1); right, top, bottom: outflow (type 2);
-    obstacle surface: diffuse wall (type 4)."""
+    removed.  Left: inflow (type 1); right: outflow (type 2); top and
+    bottom: outflow (sides="outflow"), free stream (sides="freestream",
+    type 1: the INFLOW reset holds them at the inflow Maxwellian) or diffuse
+    walls (sides="wall", type 4); obstacle surface: diffuse wall (type 4).
+
+    A zero-gradient side parallel to the stream neither damps nor fixes a
+    transverse disturbance, so with outflow sides the steady state the march
+    reaches depends on where it started; free-stream sides pin it."""
+    if sides not in ("outflow", "freestream", "wall"):
+        raise ValueError("sides: 'outflow', 'freestream' or 'wall'")
     hx = (x1 - x0) / nx
     hy = (y1 - y0) / ny
     xc = x0 + (np.arange(nx) + 0.5) * hx
@@ -146,13 +154,15 @@ def channel_mesh(x0, x1, y0, y1, nx, ny, obstacle_side=1.0, center=(0.0, 0.0)):
     def st(kind, outside, i, j):
         if not outside:
             return 4
+        if kind in ("top", "bottom") and sides != "outflow":
+            return 1 if sides == "freestream" else 4
         return 1 if kind == "left" else 2
 
     intma, coord, bsido = _grid_mesh(x0, x1, y0, y1, nx, ny, active, st)
     side = float(inside.any(axis=0).sum() * hx)
     return RawMesh(intma, coord, bsido, None,
                    {"kind": "channel", "nx": nx, "ny": ny, "obstacle_cells": int(inside.sum()),
-                    "obstacle_side": side})
+                    "obstacle_side": side, "sides": sides})
 
 
 def physical_params(mach, kn, length=1.0, rho=1.0, temp=1.0, rgas=1.0):
@@ -202,11 +212,12 @@ def cavity_case(n=32, nr=16, nt=32, mach=0.3, kn=0.1, perturb=1e-3, seed=0):
 
 
 def channel_case(x0=-5.0, x1=15.0, y0=-5.0, y1=5.0, nx=200, ny=100, nr=24, nt=48, mach=2.0, kn=0.05,
-                 obstacle_side=1.0):
+                 obstacle_side=1.0, sides="outflow"):
     """Supersonic channel flow past a square obstacle; the domain starts at
-    the free-stream Maxwellian (INICON2 with U0 = U)."""
+    the free-stream Maxwellian (INICON2 with U0 = U).  `sides`: the top and
+    bottom boundary type (channel_mesh)."""
     ph = physical_params(mach, kn, length=obstacle_side)
-    mesh = channel_mesh(x0, x1, y0, y1, nx, ny, obstacle_side)
+    mesh = channel_mesh(x0, x1, y0, y1, nx, ny, obstacle_side, sides=sides)
     rv = 4.0 * math.sqrt(ph["rgas"] * ph["temp"]) + ph["speed"]
     cinf = (ph["temp"], ph["p_bar"], ph["speed"], 0.0)
     return CaseDef(name=f"channel{nx}x{ny}_v{nr}x{nt}", mesh=mesh, rorder=nr, torder=nt, rv=rv, rgas=ph["rgas"],

@@ -152,7 +152,9 @@ template <class T> int sweep_per_sm(int eb, int immat, int max_halo, bool one) {
   SweepFn<T> fn = sweep_fn<T>(eb, immat, one);
   if (allow_max_smem((const void*)fn) != 0) return 0;
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)fn, 2 * eb, smem) != cudaSuccess) return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)fn, SweepGeo<T>::TPE * eb, smem) !=
+      cudaSuccess)
+    return 0;
   return per_sm;
 }
 
@@ -280,9 +282,10 @@ template <class T> int enqueue_step(const LaunchSet<T>& L, cudaStream_t st, floa
     TRY(launch_check("k_wall", (L.total_walls + 7) / 8, 256, 0));
   }
   if (ms) cudaEventRecord(ev[2], st);
-  sweep_fn<T>(L.eb, L.immat, L.one)<<<L.sweep_grid, 2 * L.eb, L.sweep_smem, st>>>(L.args, L.total_units,
-                                                                                   L.one_case);
-  TRY(launch_check("k_sweep", L.sweep_grid, 2 * L.eb, L.sweep_smem));
+  constexpr int TPE = SweepGeo<T>::TPE;
+  sweep_fn<T>(L.eb, L.immat, L.one)<<<L.sweep_grid, TPE * L.eb, L.sweep_smem, st>>>(L.args, L.total_units,
+                                                                                     L.one_case);
+  TRY(launch_check("k_sweep", L.sweep_grid, TPE * L.eb, L.sweep_smem));
   if (ms) cudaEventRecord(ev[3], st);
   k_resid<T><<<L.n, 32, 0, st>>>(L.args);
   TRY(launch_check("k_resid", L.n, 32, 0));
@@ -514,7 +517,7 @@ template <class T> struct Impl : ImplBase {
     return 0;
   }
 
-  // Sweep tile: EB elements per CTA (2*EB threads) x one 64-byte velocity
+  // Sweep tile: EB elements per CTA (TPE*EB threads) x one 64-byte velocity
   // segment; `upc` work units per resident CTA picks the tiles per unit.
   int set_tile(int tile_elems, int upc) {
     const int eb = tile_elems > 0 ? tile_elems : default_eb();

@@ -468,6 +468,20 @@ template <class T> struct SweepGeo {
   static constexpr int W = 16 / (int)sizeof(T);  // values per 16-byte vector
   static constexpr int VT = 64 / (int)sizeof(T);  // velocities per tile
   static constexpr int NCH = 4;                   // 16-byte chunks per row segment
+  // threads per block element in the sweep, each taking NCH / TPE chunks.
+  // Two for both precisions: on the Mach 2 channel (200x100, 24x48) four
+  // threads per element made the FP32 sweep 0.42 -> 0.55 ms, and the FP64
+  // sweep (16 warps per SM but 128 registers, spilling) slower than two
+  // threads at 8 warps and 226 registers without spills
+#ifndef DGBGK_SWEEP_TPE32
+#define DGBGK_SWEEP_TPE32 2
+#endif
+#ifndef DGBGK_SWEEP_TPE64
+#define DGBGK_SWEEP_TPE64 2
+#endif
+  static constexpr int TPE = sizeof(T) == 4 ? DGBGK_SWEEP_TPE32 : DGBGK_SWEEP_TPE64;
+  static constexpr int CPT = NCH / TPE;           // chunks per thread
+  static_assert(TPE == 2 || TPE == 4, "two or four threads per element");
   static constexpr int BOX_ROWS = 192;            // rows of one TMA box
   static constexpr int RW = (int)(sizeof(ElemRec<T>) / 16);                    // record words
   static constexpr int HW = (REC_HEAD_VALUES * (int)sizeof(T) + 15) / 16;        // head words
@@ -608,7 +622,7 @@ __device__ __forceinline__ void sweep_p1(const ElemRec<T>& r, unsigned char* tl,
   for (int i = 0; i < 3; ++i) vst<T>(row[i], f[i]);
 }
 
-// Persistent sweep kernel: EB block elements, 2*EB threads.  Work units are
+// Persistent sweep kernel: EB block elements, TPE*EB threads.  Work units are
 // (block b, group of `tpu` velocity tiles) with b fastest, handed out in
 // order (the first by blockIdx, the rest from a device counter), so the CTAs
 // running at one moment cover neighbouring blocks at the same velocities and
@@ -620,8 +634,8 @@ __device__ __forceinline__ void sweep_p1(const ElemRec<T>& r, unsigned char* tl,
 //  * phase 1: UMEAN and g = f - UMEAN of every block and halo element; a
 //    block element's NFO and UMEAN stay in the registers of the thread that
 //    updates it;
-//  * phase 2, thread j and j+EB take half of block element j's velocities
-//    each: the volume term (src/getelc.f90:87-117), the edge fluxes gathered
+//  * phase 2, threads j, j+EB, .. (TPE of them) take NCH/TPE of block
+//    element j's 16-byte velocity chunks each: the volume term (src/getelc.f90:87-117), the edge fluxes gathered
 //    per element (EDGFLXOPT src/edgflxopt.f90:95-125; outflow and, with zero
 //    length, inflow and wall sides read the element itself), the wall sides'
 //    fluxes (GETBOU src/getbou.f90:142-281), GETINC/CMMINC, ADTHEM and INFLOW;
@@ -632,13 +646,14 @@ __device__ __forceinline__ void sweep_p1(const ElemRec<T>& r, unsigned char* tl,
 // it where SC > 0 for the ISIDE(3) element and SC >= 0 for the other; the
 // two differ only at SC = 0, where the flux SC*value is zero either way.
 template <class T, int EB, int IMMAT, bool ONE>
-__global__ void __launch_bounds__(2 * EB, sizeof(T) == 4 ? 2 : 1)
+__global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : 1)
     k_sweep(BatchArgs<T> a, int total_units, const __grid_constant__ CaseDev<T> one) {
   using G = SweepGeo<T>;
   using VO = Vec<T>;
   using VecT = typename VO::type;
   constexpr int W = G::W, VT = G::VT, NCH = G::NCH, RW = G::RW, HW = G::HW, HR = G::HR;
-  constexpr int NT = 2 * EB, NW = NT / 32;
+  constexpr int TPE = G::TPE, CPT = G::CPT;
+  constexpr int NT = TPE * EB, NW = NT / 32;
   constexpr int NBOX = (3 * EB + G::BOX_ROWS - 1) / G::BOX_ROWS;
   constexpr unsigned BOX_BYTES = G::BOX_ROWS * 64;
   static_assert(EB % 16 == 0, "whole warps");
@@ -655,7 +670,7 @@ __global__ void __launch_bounds__(2 * EB, sizeof(T) == 4 ? 2 : 1)
   T* const vtab = reinterpret_cast<T*>(hrec + (size_t)a.max_halo * HR);  // cx, cy, NFINF
   constexpr int UV = G::TPU_MAX * VT;
   int* const hl = reinterpret_cast<int*>(vtab + 3 * UV);  // halo elements of the unit's block
-  const int j = tid < EB ? tid : tid - EB, hh = tid < EB ? 0 : 1;
+  const int j = tid % EB, hh = tid / EB;  // block element, and which of its TPE parts
   const T third = (T)(1.0 / 3.0);
   if (tid == 0) {
     mbar_init(&bars[0], 1);
@@ -762,13 +777,14 @@ __global__ void __launch_bounds__(2 * EB, sizeof(T) == 4 ? 2 : 1)
         const T* vy = vtab + UV + k * VT;
         const T* vn = vtab + 2 * UV + k * VT;
 
-        // ---- phase 1: block element j (half hh), then the halo chunk by chunk
-        VecT qr[2][3], ur[2];
+        // ---- phase 1: block element j (chunks CPT*hh ..), then the halo
+        // chunk by chunk
+        VecT qr[CPT][3], ur[CPT];
         if (j < nb) {
           const ElemRec<T>& r = recs[j];
 #pragma unroll
-          for (int cc = 0; cc < 2; ++cc) {
-            const int cq = 2 * hh + cc;
+          for (int cc = 0; cc < CPT; ++cc) {
+            const int cq = CPT * hh + cc;
             sweep_p1<T>(r, tl, 3 * j, cq, vld<T>(vx + cq * W), vld<T>(vy + cq * W), dth, dth3, qr[cc], ur[cc]);
           }
         }
@@ -785,13 +801,15 @@ __global__ void __launch_bounds__(2 * EB, sizeof(T) == 4 ? 2 : 1)
           cp_async_commit();
         }
 
-        // ---- phase 2: the update of block element j, half hh.  Row offsets
-        // are taken at chunk 2*hh; chunk 2*hh+1 of the same row is at offset ^ 16.
+        // ---- phase 2: the update of block element j, chunks CPT*hh ..
+        // CPT*hh + CPT - 1.  Row offsets are taken at chunk CPT*hh; chunk
+        // CPT*hh + cc of the same row is at offset ^ 16*cc (CPT*hh is a
+        // multiple of CPT, so CPT*hh + cc = CPT*hh ^ cc).
         T rmt = (T)0, sqt = (T)0;
         unsigned own[3];
 #pragma unroll
-        for (int i = 0; i < 3; ++i) own[i] = tile_off(3 * j + i, 2 * hh);
-        VecT outv[2][3];
+        for (int i = 0; i < 3; ++i) own[i] = tile_off(3 * j + i, CPT * hh);
+        VecT outv[CPT][3];
         if (j < nb) {
           const ElemRec<T>& r = recs[j];
           const int e = e0 + j;
@@ -814,16 +832,16 @@ __global__ void __launch_bounds__(2 * EB, sizeof(T) == 4 ? 2 : 1)
           for (int k2 = 0; k2 < 3; ++k2) {
             const int inf = r.edge[k2].info, kind = inf & 3;
             const int r0 = 3 * (inf >> 8);
-            srcp[k2] = tile_off(r0 + ((inf >> 3) & 3), 2 * hh);
-            srcq[k2] = tile_off(r0 + ((inf >> 5) & 3), 2 * hh);
+            srcp[k2] = tile_off(r0 + ((inf >> 3) & 3), CPT * hh);
+            srcq[k2] = tile_off(r0 + ((inf >> 5) & 3), CPT * hh);
             const T al = (kind == 0 || kind == 2) ? r.edge[k2].alen : (T)0;
             anx[k2] = al * r.edge[k2].nx;
             any[k2] = al * r.edge[k2].ny;
           }
           const int flags = r.flags;
 #pragma unroll
-          for (int cc = 0; cc < 2; ++cc) {
-            const int cq = 2 * hh + cc;
+          for (int cc = 0; cc < CPT; ++cc) {
+            const int cq = CPT * hh + cc;
             const unsigned cx16 = 16u * cc;
             const int vb = vb0 + cq * W;
             VecT(&out)[3] = outv[cc];
@@ -954,7 +972,7 @@ __global__ void __launch_bounds__(2 * EB, sizeof(T) == 4 ? 2 : 1)
         __syncthreads();
         if (j < nb) {
 #pragma unroll
-          for (int cc = 0; cc < 2; ++cc)
+          for (int cc = 0; cc < CPT; ++cc)
 #pragma unroll
             for (int i = 0; i < 3; ++i) vst<T>(tl + (own[i] ^ (16u * cc)), outv[cc][i]);
         }

@@ -1,0 +1,116 @@
+"""The warm-start path on the GPU: precision handoff, per-case batch status,
+and what the trained network gains over a cold start.
+
+The cases are the warm-start family's channel (free-stream sides, 100 x 100
+quads) on a 12 x 24 velocity grid, drawn from the middle of the family's
+ranges, so that a test marches in seconds (an 8 x 16 grid is too coarse: the
+explicit scheme diverges on it).  The cold FP64 march is the judge: a
+warm-started (or FP32-started) march must end, at the same residual, on the
+same fields.
+"""
+import numpy as np
+import pytest
+
+from dgbgk import Batch, Solver, channel_case
+from dgbgk._lib import DGBGK_ENONFINITE
+from dgbgk.study import FAMILY, WarmStart, cold_reference, draw_cases, generate, nodal_fields, rel_fields
+from helpers import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+SMALL = dict(FAMILY, nr=12, nt=24, mach=(2.2, 2.8), kn=(0.06, 0.12))
+
+
+def family_case(m, kn, side=1.0):
+    x0, x1, y0, y1 = FAMILY["box"]
+    return channel_case(x0, x1, y0, y1, FAMILY["nx"], FAMILY["ny"], 12, 24, mach=m, kn=kn, obstacle_side=side,
+                        sides="freestream")
+
+
+def cold(case, prec, tol, ref=None, max_steps=60000):
+    s = Solver.from_case(case, precision=prec)
+    s.init_case()
+    if ref is not None:
+        s.set_residual_reference(ref)
+    r = s.advance(max_steps, tol=tol)
+    return s, r
+
+
+def test_copy_state_converts_precision_and_keeps_the_reference():
+    c = family_case(2.5, 0.07)
+    s64, _ = cold(c, 64, 0.0, max_steps=30)
+    s32 = Solver.from_case(c, precision=32)
+    s32.copy_state_from(s64)
+    assert s32.residual_reference() == s64.residual_reference()
+    a = s64.get_state()
+    assert np.array_equal(s32.get_state(np.float32), a.astype(np.float32))
+    back = Solver.from_case(c, precision=64)
+    back.copy_state_from(s32)
+    assert np.array_equal(back.get_state(), a.astype(np.float32).astype(np.float64))
+    # same precision: an exact copy
+    twin = Solver.from_case(c, precision=64)
+    twin.copy_state_from(s64)
+    assert np.array_equal(twin.get_state(), a)
+    for s in (s64, s32, back, twin):
+        s.close()
+
+
+def test_fp32_transient_fp64_finish_matches_fp64():
+    c = family_case(2.5, 0.07)
+    ref = cold_reference(c)
+    plain, r = cold(c, 64, 1e-8, ref)
+    assert r["steps"] < 60000
+    s32, r32 = cold(c, 32, 1e-4, ref)
+    s64 = Solver.from_case(c, precision=64)
+    s64.copy_state_from(s32)
+    r64 = s64.advance(60000, tol=1e-8)
+    assert r64["res_l2"][-1] <= 1e-8 * ref * (1 + 1e-9)
+    e = rel_fields(nodal_fields(s64, c), nodal_fields(plain, c))
+    assert max(e["n"], e["u"], e["T"]) <= 1e-6
+    for s in (plain, s32, s64):
+        s.close()
+
+
+def test_batch_reports_a_diverging_case_and_finishes_the_rest():
+    # the zero-gradient-sided channel at Kn = 1 diverges within a few hundred
+    # steps (the explicit scheme's stability limit; the oracle diverges on
+    # it too); the cavity next to it must run on untouched
+    from dgbgk import cavity_case
+    bad = channel_case(-5, 15, -5, 5, 40, 20, 8, 16, mach=2.0, kn=1.0, obstacle_side=1.0)
+    good = cavity_case(8, 8, 16, mach=0.3, kn=0.1)
+    ss = [Solver.from_case(x, precision=32) for x in (bad, good)]
+    for s in ss:
+        s.init_case()
+    b = Batch(ss, tune_steps=1)
+    r = b.advance(1500, raise_on_error=False)
+    assert r["status"][0] == DGBGK_ENONFINITE and r["steps"][0] < 1500
+    assert r["status"][1] == 0 and r["steps"][1] == 1500
+    alone = Solver.from_case(good, precision=32)
+    alone.init_case()
+    alone.advance(1500)
+    assert rel_l2(ss[1].get_state(), alone.get_state()) <= 1e-6
+    with pytest.raises(Exception):
+        b.advance(10)
+    b.close()
+    alone.close()
+
+
+def test_trained_network_gains_over_the_cold_start():
+    train = draw_cases(24, 11, family=SMALL)
+    X, Y, keep = generate(train, tol=1e-4, accept=1e-3)
+    assert len(keep) >= 20
+    ws = WarmStart(width=256, depth=3, batch=128, seed=1)
+    hist = ws.fit(X, Y, schedule=((1500, 1e-3), (500, 3e-4)))
+    assert hist[-20:].mean() < 0.1 * hist[:5].mean()
+    test = draw_cases(1, 12, family=SMALL)[0]
+    ref = cold_reference(test)
+    plain, r_cold = cold(test, 64, 1e-8, ref)
+    warm = Solver.from_case(test, precision=64)
+    ws.warm([warm], [test])
+    warm.set_residual_reference(ref)
+    r_warm = warm.advance(60000, tol=1e-8)
+    assert r_warm["steps"] < 0.9 * r_cold["steps"], (r_warm["steps"], r_cold["steps"])
+    e = rel_fields(nodal_fields(warm, test), nodal_fields(plain, test))
+    assert max(e["n"], e["u"], e["T"]) <= 1e-6
+    plain.close()
+    warm.close()

@@ -7,6 +7,10 @@ supersonic channel: [-5,15]x[-5,5] as 200x100 quads (39 800 P1 triangles)
 minus a unit-square obstacle, 24 x 48 velocities (1.3755e8 DOFs), Mach 2,
 Kn 0.05, f stored in FP32 with FP64 moments and residual norms.  The metric
 is DOF-updates/s = 3*NELEM*VNPNT*steps / device time of the time loop.
+Beside it (one GPU): the plain FP64 path on the same workload, the time to
+steady state (L2 residual 1e-8) of eight warm-start-family channels plain
+FP64 vs batched FP64 vs batched FP32 with an FP64 finish, the end-to-end
+rate through the C ABI with host buffers, and the oracle on the host cores.
 
 Arms:
   --impl ours       : the sm_100a library through its C ABI.
@@ -186,7 +190,11 @@ def cpu_threads():
         return os.cpu_count() or 1
 
 
-def oracle_step_rate(case, nsteps, threads, warmup=0):
+def oracle_step_rate(case, nsteps, threads, warmup=0, min_seconds=0.0):
+    """DOF-updates/s of the oracle's time step on the host cores: nsteps
+    steps, or (min_seconds > 0) one timed step and then as many more as
+    bring the sample to about min_seconds.  Returns the rate, the seconds
+    and the steps timed."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     from pyoracle import Oracle
     o = Oracle.from_case(case, prec=32, threads=threads)
@@ -197,8 +205,14 @@ def oracle_step_rate(case, nsteps, threads, warmup=0):
     t = time.perf_counter()
     o.advance(nsteps)
     dt = time.perf_counter() - t
+    if min_seconds > 0 and dt < min_seconds:
+        more = max(1, int(min_seconds / max(dt / nsteps, 1e-9)) - nsteps)
+        t = time.perf_counter()
+        o.advance(more)
+        dt += time.perf_counter() - t
+        nsteps += more
     o.close()
-    return case.dofs * nsteps / dt, dt
+    return case.dofs * nsteps / dt, dt, nsteps
 
 
 # ------------------------------------------------------------- our arm ----
@@ -266,30 +280,23 @@ def run_ours(a, d):
                        "kernel_ms": dict(zip(names, [float(x) for x in k64]))}
         out["fp32_over_fp64_per_step"] = out["value"] / out["fp64"]["value"]
         del s64
-    # time to steady state (L2 residual 1e-8 of the first step's), cold
-    # start, plain FP64 vs FP32, on a 16^2 lid-driven cavity (16x32
-    # velocities), small enough to converge within the bench
-    if not a.no_steady:
-        from dgbgk import cavity_case
-        from dgbgk.steady import cold_march
-        sc = cavity_case(16, 16, 32, mach=0.3, kn=0.1)
-        st = {"case": sc.name, "dofs": sc.dofs, "tol": 1e-8, "start": "cold (rest Maxwellian, seeded 1e-3 "
-              "density perturbation)"}
-        for prec in (64, 32):
-            r, so = cold_march(sc, prec, 1e-8, 3000000, device=d.local)
-            r["device_s"] = d.max(r["device_s"])
-            st[f"fp{prec}"] = {k: r[k] for k in ("steps", "device_s", "res_rel", "converged")}
-            if prec == 64:
-                m64 = so.macros()
-            else:
-                m32 = so.macros()
-            del so
-        st["fp32_speedup"] = st["fp64"]["device_s"] / st["fp32"]["device_s"]
-        st["fp32_vs_fp64_rel_l2"] = {k: float(np.linalg.norm(m32[k] - m64[k]) / max(np.linalg.norm(m64[k]), 1e-300))
-                                     for k in ("rho", "temp")}
-        vs = float(np.sqrt(sc.rgas * sc.init["T1"]))  # velocities on the thermal-speed scale
-        for k in ("u", "v"):
-            st["fp32_vs_fp64_rel_l2"][k] = float(np.linalg.norm(m32[k] - m64[k]) / (vs * np.sqrt(len(m64[k]))))
+    # time to steady state (L2 residual 1e-8 of a cold start's first step)
+    # on eight channels of the warm-start family, three ways: plain FP64 one
+    # case at a time; FP64 in one batch; FP32 in one batch until 1e-5 (or
+    # its rounding plateau), then FP64 to 1e-8 (the precision handoff).  The
+    # network's share is measured by dgbgk.study (results/).
+    if not a.no_steady and d.world == 1:
+        from dgbgk.study import draw_cases, evaluate
+        cases = draw_cases(8, 77)
+        res, _, kept = evaluate(cases, None, ways=("plain", "batch64", "fast_cold"), device=d.local)
+        st = {"cases": f"{len(kept)} channels [-5,15]x[-10,10], 100x100 quads, 16x32 velocities, free-stream "
+                       "sides, Mach/Kn/obstacle drawn (dgbgk.study.draw_cases(8, 77))",
+              "dofs_per_case": kept[0].dofs if kept else 0, "tol": 1e-8, "switch_tol": res["switch_tol"],
+              "plain_fp64_s": res["plain"]["wall_s"], "plain_fp64_steps": int(sum(res["plain"]["steps"]))}
+        for k in ("batch64", "fast_cold"):
+            st[k] = {"wall_s": res[k]["wall_s"], "speedup_vs_plain": res[k]["speedup_vs_plain"],
+                     "steps": int(sum(res[k]["steps"])), "steps_fp64_finish": int(sum(res[k]["steps_fp64_finish"])),
+                     "max_rel_l2_vs_plain": res[k]["max_rel_l2_vs_plain"]}
         out["steady_state"] = st
     # end to end through the C ABI with host buffers
     if not a.no_e2e:
@@ -314,9 +321,9 @@ def run_ours(a, d):
         del s
     if d.rank == 0 and d.world == 1 and not a.no_cpu:
         thr = cpu_threads()
-        rate, secs = oracle_step_rate(case, 1, thr)
+        rate, secs, n = oracle_step_rate(case, 1, thr, min_seconds=15.0)
         out["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": thr, "kind": "port",
-                               "sample": f"1 full pseudo-time step of {case.name} (FP32, {secs:.1f} s, "
+                               "sample": f"{n} full pseudo-time steps of {case.name} (FP32, {secs:.1f} s, "
                                          f"{thr} OpenMP threads)"}
     return out
 
@@ -326,7 +333,7 @@ def run_reference(a, d):
         return None
     case = make_case(a.config)
     thr = cpu_threads()
-    rate, secs = oracle_step_rate(case, a.steps, thr, warmup=a.warmup)
+    rate, secs, _ = oracle_step_rate(case, a.steps, thr, warmup=a.warmup)
     return {"impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": d.world,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": secs * 1e3 / a.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",

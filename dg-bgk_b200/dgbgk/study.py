@@ -18,6 +18,7 @@ start) four ways:
                residual reaches `switch_tol` (or the FP32 rounding plateau),
                then the state is handed to FP64 handles (dgbgk_copy_state)
                and the batch finishes to 1e-8
+  fast_cold    as fast, from the cold start (no network)
 
 A stored FP32 state stops changing once every update is below half an ulp,
 so an FP32 march settles anywhere within about tau * ulp / 2 of its fixed
@@ -211,9 +212,9 @@ class WarmStart:
         return grids
 
 
-def cold_reference(case):
+def cold_reference(case, device=0):
     """The L2 residual of the first FP64 step from the cold start."""
-    s = Solver.from_case(case, precision=64)
+    s = Solver.from_case(case, precision=64, device=device)
     s.init_case()
     s.advance(1)
     r = s.residual_reference()
@@ -228,11 +229,11 @@ def rel_fields(a, b):
 
 
 def evaluate(cases, ws, tol=1e-8, switch_tol=1e-5, max_steps=200000,
-             ways=("plain", "batch64", "batch64_warm", "fast"), log=None):
+             ways=("plain", "batch64", "batch64_warm", "fast"), log=None, device=0):
     """Time to tol for each way (see the module docstring); returns the
     results, the final normalised nodal fields per way and the cases kept."""
     from ._lib import DgbgkError
-    refs = [cold_reference(c) for c in cases]
+    refs = [cold_reference(c, device) for c in cases]
     out = {"ncases": len(cases), "tol": tol, "switch_tol": switch_tol}
     final = {}
 
@@ -241,7 +242,7 @@ def evaluate(cases, ws, tol=1e-8, switch_tol=1e-5, max_steps=200000,
         # every comparison
         steps, dev, wall, fields, kept = [], 0.0, 0.0, [], []
         for i, (c, ref) in enumerate(zip(cases, refs)):
-            s = Solver.from_case(c, precision=64)
+            s = Solver.from_case(c, precision=64, device=device)
             s.init_case()
             s.set_residual_reference(ref)
             t = time.perf_counter()
@@ -270,8 +271,8 @@ def evaluate(cases, ws, tol=1e-8, switch_tol=1e-5, max_steps=200000,
 
     def batched(name, warm, precision_first, switch):
         t0 = time.perf_counter()
-        first = [Solver.from_case(c, precision=precision_first) for c in cases]
-        fin = [Solver.from_case(c, precision=64) for c in cases] if switch else first
+        first = [Solver.from_case(c, precision=precision_first, device=device) for c in cases]
+        fin = [Solver.from_case(c, precision=64, device=device) for c in cases] if switch else first
         t_setup = time.perf_counter() - t0
         t = time.perf_counter()
         if warm:
@@ -333,6 +334,8 @@ def evaluate(cases, ws, tol=1e-8, switch_tol=1e-5, max_steps=200000,
         out["batch64_warm"] = batched("batch64_warm", True, 64, None)
     if "fast" in ways:
         out["fast"] = batched("fast", True, 32, switch_tol)
+    if "fast_cold" in ways:
+        out["fast_cold"] = batched("fast_cold", False, 32, switch_tol)
     if "plain" in final:
         for k in final:
             if k == "plain":

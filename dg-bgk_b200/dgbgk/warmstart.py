@@ -80,3 +80,42 @@ class MLP:
         hist = np.zeros(iters)
         check(lib().dgbgk_mlp_train(self._h, iters, lr, seed, ptr(hist)))
         return hist
+
+
+def main(argv=None):
+    """Training throughput of the network on synthetic data:
+
+        python -m dgbgk.warmstart --batch 1024 --iters 50
+
+    prints the Adam steps per second and the tensor-core FLOP rate of the
+    GEMMs (6 * batch * sum of layer in*out FLOPs per step: forward, and the
+    weight and input gradients)."""
+    import argparse
+    import json
+    import time
+    ap = argparse.ArgumentParser(description="warm-start network training throughput")
+    ap.add_argument("--width", type=int, default=512)
+    ap.add_argument("--depth", type=int, default=4)
+    ap.add_argument("--n-out", type=int, default=32768)
+    ap.add_argument("--batch", type=int, default=256)
+    ap.add_argument("--iters", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=3)
+    a = ap.parse_args(argv)
+    m = MLP(3, a.width, a.depth, a.n_out, a.batch, seed=0)
+    rng = np.random.default_rng(0)
+    x = rng.uniform(-1, 1, (4 * a.batch, 3)).astype(np.float32)
+    t = rng.normal(0, 1, (4 * a.batch, a.n_out)).astype(np.float32)
+    m.set_data(x, t)
+    m.train(a.warmup, lr=1e-4)
+    t0 = time.perf_counter()
+    m.train(a.iters, lr=1e-4)
+    dt = time.perf_counter() - t0
+    layers = [(64, a.width)] + [(a.width, a.width)] * (a.depth - 1) + [(a.width, a.n_out)]
+    flops = 6.0 * a.batch * sum(i * o for i, o in layers) * a.iters
+    print(json.dumps({"batch": a.batch, "params": m.param_count(), "iters": a.iters, "ms_per_iter": 1e3 * dt / a.iters,
+                      "gemm_tflops": flops / dt / 1e12}))
+    m.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -106,6 +106,7 @@ template <class T> struct LaunchSet {
   int eb = 128, immat = 1;
   bool one = false;       // a single case: the kernels take it as a parameter
   CaseDev<T> one_case{};  // that case (zeros for a batch)
+  std::vector<CaseDev<T>> spec_cases;  // cases with ALPHA < 1 wall sides (k_wspec runs per case)
   int mom_rows = 1, mom_warps = 1, mom_grid = 1, sweep_grid = 1;
   size_t mom_smem = 0, sweep_smem = 0;
   ~LaunchSet() { release(); }
@@ -176,6 +177,9 @@ int build_launch_set(LaunchSet<T>& L, const std::vector<CaseDev<T>>& cs, int eb,
                      cudaStream_t st, int force_rows = 0) {
   const int n = (int)cs.size();
   const bool one = n == 1;
+  L.spec_cases.clear();
+  for (const auto& c : cs)
+    if (c.spec) L.spec_cases.push_back(c);
   unsigned maxrow = 16;
   for (const auto& c : cs) maxrow = std::max(maxrow, c.rowbytes);
   // one case: its moment tables sit in shared memory
@@ -286,6 +290,20 @@ template <class T> int enqueue_step(const LaunchSet<T>& L, cudaStream_t st, floa
   sweep_fn<T>(L.eb, L.immat, L.one)<<<L.sweep_grid, TPE * L.eb, L.sweep_smem, st>>>(L.args, L.total_units,
                                                                                      L.one_case);
   TRY(launch_check("k_sweep", L.sweep_grid, TPE * L.eb, L.sweep_smem));
+  // the specular part of ALPHA < 1 wall sides: the parallel items, then the
+  // ones that wait on earlier deferred velocities
+  for (const auto& c : L.spec_cases) {
+    if (c.n_spec_par > 0) {
+      const int g = std::min(4 * 148, (c.n_spec_par + 255) / 256);
+      k_wspec<T><<<g, 256, 0, st>>>(c, 0);
+      TRY(launch_check("k_wspec", g, 256, 0));
+    }
+    if (c.spec_seq) {
+      const int g = (c.n_spec_slots + 255) / 256;
+      k_wspec<T><<<g, 256, 0, st>>>(c, 1);
+      TRY(launch_check("k_wspec", g, 256, 0));
+    }
+  }
   if (ms) cudaEventRecord(ev[3], st);
   k_resid<T><<<L.n, 32, 0, st>>>(L.args);
   TRY(launch_check("k_resid", L.n, 32, 0));
@@ -327,6 +345,10 @@ template <class T> struct Impl : ImplBase {
   void* staging = nullptr;
   size_t staging_bytes = 0;
   int* d_inv = nullptr;
+  // ALPHA < 1 wall sides
+  int *rside = nullptr, *rf_i = nullptr, *welem = nullptr, *spec_par = nullptr, *spec_seq_off = nullptr,
+      *spec_seq = nullptr;
+  T *rf_z = nullptr, *wd = nullptr;
   CaseDev<T> hc;          // this case's table entry
   LaunchSet<T> single;    // this case alone
 
@@ -367,6 +389,14 @@ template <class T> struct Impl : ImplBase {
     dfree(hist_l2);
     dfree(hist_dt);
     dfree(ctrl);
+    dfree(rside);
+    dfree(rf_i);
+    dfree(rf_z);
+    dfree(welem);
+    dfree(wd);
+    dfree(spec_par);
+    dfree(spec_seq_off);
+    dfree(spec_seq);
     if (staging) cudaFree(staging);
     if (hctrl) cudaFreeHost(hctrl);
     if (ev0) cudaEventDestroy(ev0);
@@ -431,6 +461,18 @@ template <class T> struct Impl : ImplBase {
     TRY(upload(&node_off, pl.node_off, st));
     TRY(upload(&node_dg, pl.node_dg, st));
     TRY(upload(&node_ae, pl.node_ae, st));
+    if (pl.spec) {
+      std::vector<T> rz(pl.rf_z.begin(), pl.rf_z.end());
+      TRY(upload(&rside, pl.rside, st));
+      TRY(upload(&rf_i, pl.rf_i, st));
+      TRY(upload(&rf_z, rz, st));
+      TRY(upload(&welem, pl.welem, st));
+      TRY(dalloc(&wd, std::max<size_t>(1, pl.welem.size() * 3 * (size_t)Vp)));
+      std::vector<int> one1(1, 0);
+      TRY(upload(&spec_par, pl.spec_par.empty() ? one1 : pl.spec_par, st));
+      TRY(upload(&spec_seq_off, pl.spec_seq_off, st));
+      if (!pl.spec_seq.empty()) TRY(upload(&spec_seq, pl.spec_seq, st));
+    }
     TRY(dalloc(&ctrl, 1));
     CK(cudaMallocHost((void**)&hctrl, 3 * sizeof(Ctrl)));
     std::memset(hctrl, 0, 3 * sizeof(Ctrl));
@@ -507,6 +549,17 @@ template <class T> struct Impl : ImplBase {
     hc.tpu = tpu;
     hc.nwall = (int)pl.walls.size();
     hc.rowbytes = (unsigned)(((size_t)pl.V * sizeof(T) + 15) / 16 * 16);
+    hc.spec = pl.spec ? 1 : 0;
+    hc.n_spec_par = (int)pl.spec_par.size();
+    hc.n_spec_slots = (int)pl.welem.size();
+    hc.rside = rside;
+    hc.rf_i = rf_i;
+    hc.rf_z = rf_z;
+    hc.welem = welem;
+    hc.wd = wd;
+    hc.spec_par = spec_par;
+    hc.spec_seq_off = spec_seq_off;
+    hc.spec_seq = spec_seq;
   }
 
   // the one-case launch set
@@ -554,6 +607,7 @@ template <class T> struct Impl : ImplBase {
         }
         r[e].area = (T)g.area;
         r[e].flags = flags;
+        r[e].wslot = pl.spec ? pl.wslot[e] : -1;
       }
       TRY(upload(&rec, r, st));
     }
@@ -986,10 +1040,6 @@ int dgbgk_create(const dgbgk_mesh* mesh, const dgbgk_vspace* vs, const dgbgk_par
   if (rc != 0) {
     set_error(err);
     return rc;
-  }
-  if (impl->pl.alpha != 1.0 && impl->pl.has_wall_incoming) {
-    set_error("dgbgk_create: wall accommodation ALPHA < 1 (specular part) is not supported by this build");
-    return DGBGK_EUNSUP;
   }
   if (prm->precision == 64)
     rc = static_cast<Impl<double>*>(impl.get())->init(eb0);

@@ -149,6 +149,17 @@ template <class T> struct alignas(64) CaseDev {
   int E, V, Vp, nblocks, nvt, tpu;
   int nwall;          // FLUCON2 wall sides
   unsigned rowbytes;  // V*sizeof(T) rounded up to 16
+  // ALPHA < 1: the specular part of the wall flux (the host plan's tables)
+  int spec;                 // 0: ALPHA = 1 or no wall side
+  int n_spec_par, n_spec_slots;
+  const int* rside;         // [B] reflection-table row, -1 off the walls
+  const int* rf_i;          // [rows][V][2] mirrored grid velocities I1, I2; -1 where TEST >= 0
+  const T* rf_z;            // [rows][V][2] ZD1, ZD2
+  const int* welem;         // [slots] wall elements (plan order)
+  T* wd;                    // [slots][3][Vp] deferred DELUN without the specular part
+  const int* spec_par;      // items slot*V + v
+  const int* spec_seq_off;  // [slots + 1]
+  const int* spec_seq;
 };
 
 template <class T> struct BatchArgs {
@@ -881,9 +892,14 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : 1)
                 rhs[qn][w] -= as * (up + (T)2 * uq);
               }
             }
+            // ALPHA < 1: bit 3*w + i marks node i at velocity vb + w as
+            // deferred (its update gets the specular part in k_wspec)
+            unsigned dmask = 0u;
             if (flags & 0x38) {
               // wall sides; molecules leaving the wall (src/getbou.f90:189-255)
-              // carry the fully diffuse part ALPHA*ETA*Mw (ALPHA < 1 is not built)
+              // carry the diffuse part ALPHA*ETA*Mw here, the specular part
+              // (1-ALPHA)*Rf in k_wspec
+              const bool spec = C.spec != 0;
 #pragma unroll
               for (int k2 = 0; k2 < 3; ++k2) {
                 if (!(flags & (8 << k2))) continue;
@@ -892,12 +908,16 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : 1)
                 const T twr = (T)2 * C.rgas * C.bTw[bs];
                 const T uwx = C.bUw[2 * bs], uwy = C.bUw[2 * bs + 1], eta = C.bEta[bs];
                 const T nx = r.edge[k2].nx, ny = r.edge[k2].ny, alw = r.edge[k2].alen;
+                // with the specular part, the wall branch is taken where the
+                // host's FP64 TEST < 0 (the items of k_wspec are built from it)
+                const int* rfi = spec ? C.rf_i + (size_t)C.rside[bs] * C.V * 2 : nullptr;
 #pragma unroll
                 for (int w = 0; w < W; ++w) {
                   const T cx = VO::get(cxv, w), cy = VO::get(cyv, w);
                   const T sc = nx * cx + ny * cy;
+                  const bool own = spec ? !(vb + w < C.V && rfi[2 * (vb + w)] >= 0) : sc >= (T)0;
                   T up, uq;
-                  if (sc >= (T)0) {
+                  if (own) {
                     up = VO::get(g[p], w);
                     uq = VO::get(g[qn], w);
                   } else {
@@ -910,6 +930,7 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : 1)
                       mw = dexp<T>(-(dx * dx + dy * dy) / twr);
                     }
                     up = uq = C.alpha * (mw * eta);
+                    if (spec) dmask |= ((1u << p) | (1u << qn)) << (3 * w);
                   }
                   const T as = alw * sc;
                   rhs[p][w] -= as * ((T)2 * up + uq);
@@ -944,8 +965,14 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : 1)
                   const T ch = (fn < (T)0) ? -f : d;
                   fn = fn > (T)0 ? fn : (T)0;
                   if (live) {
-                    rmt = rr > rmt ? rr : rmt;
-                    if (!(flags & (1 << i))) sqt += ch * ch;
+                    if ((dmask >> (3 * w + i)) & 1u) {
+                      // deferred: k_wspec adds the specular part, clips and
+                      // counts the residual
+                      C.wd[((size_t)r.wslot * 3 + i) * C.Vp + vb + w] = d;
+                    } else {
+                      rmt = rr > rmt ? rr : rmt;
+                      if (!(flags & (1 << i))) sqt += ch * ch;
+                    }
                   } else {
                     fn = (T)0;
                   }
@@ -1022,6 +1049,83 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : 1)
     if (tid == 0 && unit < total_units) next = (int)gridDim.x + atomicAdd(&a.ctl->sweep_next, 1);
   }
   if (tid == 0) bulk_wait0();  // the last box stores are complete before the CTA exits
+}
+
+// ------------------------------------------------ specular wall part ----
+// GETBOU's specular part for ALPHA < 1 (src/getbou.f90:189-255, IMMAT = 1):
+// a molecule leaving wall side k of element e at velocity v carries
+// UNSID = (1-ALPHA)*Rf + ALPHA*ETA*Mw with Rf = (ZD2*f(I1) + ZD1*f(I2)) /
+// (ZD1 + ZD2) of the element's own nodes at the mirrored grid velocities.
+// The reference reads f(I) from DISNF while its velocity loop updates it in
+// place: the new value for I < v, the old one for I > v.  The sweep has
+// applied the diffuse part and stored DELUN of the deferred nodes (wd); the
+// specular part is linear in RHS, so here DELUN += MMAT*DTE*dRHS with dRHS
+// the edge term of (1-ALPHA)*Rf, then ADTHEM's clip, INFLOW's reset and the
+// residual.  seq = 0: the items whose mirrored velocities include no earlier
+// deferred one, a thread each; seq = 1: the others, one thread per wall
+// element in velocity order (after the parallel ones).
+template <class T> __global__ void __launch_bounds__(256) k_wspec(const __grid_constant__ CaseDev<T> C, int seq) {
+  if (C.ctrl->done) return;
+  const T dt = (T)step_dt(C.ctrl);
+  const int cur = C.ctrl->cur;
+  const T* __restrict__ fo = C.f[cur];
+  T* fnw = C.f[cur ^ 1];
+  const T om = (T)1 - C.alpha;
+  double mx = 0.0, sq = 0.0;
+  auto item = [&](int it) {
+    const int s = it / C.V, v = it - s * C.V;
+    const int e = C.welem[s];
+    const ElemRec<T>& r = C.rec[e];
+    const T cx = C.cx[v], cy = C.cy[v];
+    T drhs[3] = {(T)0, (T)0, (T)0};
+    unsigned mask = 0u;
+    auto F = [&](int node, int I) {
+      const size_t o = ((size_t)e * 3 + node) * C.Vp + I;
+      return I < v ? fnw[o] : fo[o];
+    };
+    for (int k = 0; k < 3; ++k) {
+      if (!(r.flags & (8 << k))) continue;
+      const size_t o = ((size_t)C.rside[r.bside[k]] * C.V + v) * 2;
+      const int i1 = C.rf_i[o], i2 = C.rf_i[o + 1];
+      if (i1 < 0) continue;
+      const T zd1 = C.rf_z[o], zd2 = C.rf_z[o + 1];
+      const int p = k, q = (k + 1) % 3;
+      const T dp = om * ((zd2 * F(p, i1) + zd1 * F(p, i2)) / (zd1 + zd2));
+      const T dq = om * ((zd2 * F(q, i1) + zd1 * F(q, i2)) / (zd1 + zd2));
+      const T as = r.edge[k].alen * (r.edge[k].nx * cx + r.edge[k].ny * cy);
+      drhs[p] -= as * ((T)2 * dp + dq);
+      drhs[q] -= as * (dp + (T)2 * dq);
+      mask |= (1u << p) | (1u << q);
+    }
+    for (int i = 0; i < 3; ++i) {
+      if (!((mask >> i) & 1u)) continue;
+      const size_t o = ((size_t)e * 3 + i) * C.Vp + v;
+      const T d = C.wd[((size_t)s * 3 + i) * C.Vp + v] + (r.mm[i] * dt) * drhs[i];
+      const T f = fo[o];
+      T f1 = f + d;
+      const T ch = (f1 < (T)0) ? -f : d;
+      f1 = f1 > (T)0 ? f1 : (T)0;
+      mx = fmax(mx, (double)fabs(d));
+      if (r.flags & (1 << i))
+        f1 = C.nfinf[v];
+      else
+        sq += (double)ch * (double)ch;
+      fnw[o] = f1;
+    }
+  };
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
+  if (!seq) {
+    for (int it = tid; it < C.n_spec_par; it += nt) item(C.spec_par[it]);
+  } else {
+    for (int s = tid; s < C.n_spec_slots; s += nt)
+      for (int j = C.spec_seq_off[s]; j < C.spec_seq_off[s + 1]; ++j) item(C.spec_seq[j]);
+  }
+  mx = warp_max(mx);
+  sq = warp_sum(sq);
+  if ((threadIdx.x & 31) == 0 && (mx > 0.0 || sq > 0.0)) {
+    atomicAdd(&C.ctrl->acc_sq, sq);
+    atomicMax(reinterpret_cast<unsigned long long*>(&C.ctrl->acc_max), (unsigned long long)__double_as_longlong(mx));
+  }
 }
 
 // ----------------------------------------------------------- residual ----

@@ -68,6 +68,137 @@ void build_blocks(Plan& pl, int EB) {
   }
 }
 
+// GETBOU's mirrored-velocity lookup (src/getbou.f90:198-242) for every wall
+// side and outgoing velocity, in FP64 as the oracle evaluates it, and the
+// item lists of the specular update (see Plan::spec).  The ring of the
+// mirrored speed is found by the reference's own formula: it compares ETAref
+// with VCORD(1, 1 + (IETA-1)*(RORDER-1)) and takes the angles of ring
+// IETA-1, which selects the right ring when RORDER = TORDER; other grids
+// follow the same formula and fail here where it leaves VCORD.
+static int build_specular(const dgbgk_mesh& m, const dgbgk_vspace& vs, Plan& pl, std::string* err) {
+  auto fail = [&](int code, const char* msg) {
+    if (err) *err = msg;
+    return code;
+  };
+  const int E = pl.E, B = pl.B, V = pl.V, RO = pl.RORDER, TO = pl.TORDER;
+  const double PI = PI_REF;
+  auto VC = [&](int row, int idx1) { return vs.vcord[3 * (size_t)(idx1 - 1) + (row - 1)]; };  // VCORD(row, idx)
+  pl.rside.assign(B, -1);
+  int rows = 0;
+  for (int b = 0; b < B; ++b) {
+    const int t = m.bsido[6 * b + 3];
+    if (t != 1 && t != 2) pl.rside[b] = rows++;
+  }
+  pl.rf_i.assign((size_t)rows * V * 2, -1);
+  pl.rf_z.assign((size_t)rows * V * 2, 0.0);
+  for (int b = 0; b < B; ++b) {
+    const int row = pl.rside[b];
+    if (row < 0) continue;
+    const double ANX = m.rsido[3 * b], ANY = m.rsido[3 * b + 1];
+    for (int v = 0; v < V; ++v) {
+      const double UX = pl.cx[v], UY = pl.cy[v];
+      const double TEST = UX * ANX + UY * ANY;
+      if (!(TEST < 0.0)) continue;
+      const double CXR = UX + std::fabs(2 * TEST) * ANX, CYR = UY + std::fabs(2 * TEST) * ANY;
+      const double RT = std::sqrt(CXR * CXR + CYR * CYR);
+      const double QUO = std::fabs(CXR / RT);
+      double THETA = std::fabs(std::acos(QUO));
+      if (CXR < 0.0) THETA = PI - THETA;
+      if (CYR < 0.0) THETA = -THETA;
+      double ETAref = ((2 * RT) / vs.rv) - 1;
+      if (ETAref > 1.0) ETAref = 1.0;
+      const double ZETAref = THETA / PI;
+      int IETA;
+      for (IETA = 1; IETA <= RO; ++IETA) {
+        const int idx = 1 + (IETA - 1) * (RO - 1);
+        if (idx < 1 || idx > V)
+          return fail(DGBGK_EUNSUP, "dgbgk_create: ALPHA < 1: the mirrored-speed lookup leaves VCORD for this "
+                                    "velocity grid (RORDER > TORDER + 1)");
+        if (std::fabs(ETAref - VC(1, idx)) < 0.0001) break;
+      }
+      const int ring = IETA - 1;
+      int IZETA, I1, I2;
+      double ZD1 = 0, ZD2 = 0;
+      bool found = false;
+      for (IZETA = 1; IZETA <= TO - 1; ++IZETA) {
+        const double Z1 = VC(2, IZETA), Z2 = VC(2, IZETA + 1);
+        ZD1 = Z2 - Z1;
+        ZD2 = ZETAref - Z1;
+        if (ZETAref >= Z1 && ZETAref <= Z2) {
+          found = true;
+          break;
+        }
+      }
+      if (found) {
+        I1 = (ring - 1) * TO + IZETA;
+        I2 = (ring - 1) * TO + IZETA + 1;
+      } else {
+        ZD1 = VC(2, 1) - (-1.0);
+        ZD2 = ZETAref - (-1.0);
+        I1 = ring * TO;
+        I2 = (ring - 1) * TO + 1;
+      }
+      if (I1 < 1 || I1 > V || I2 < 1 || I2 > V)
+        return fail(DGBGK_EUNSUP, "dgbgk_create: ALPHA < 1: the mirrored velocity falls outside the velocity grid "
+                                  "(the reference's ring lookup needs RORDER = TORDER)");
+      const size_t o = ((size_t)row * V + v) * 2;
+      pl.rf_i[o] = I1 - 1;
+      pl.rf_i[o + 1] = I2 - 1;
+      pl.rf_z[o] = ZD1;
+      pl.rf_z[o + 1] = ZD2;
+    }
+  }
+  // wall elements and their items
+  pl.wslot.assign(E, -1);
+  pl.welem.clear();
+  for (int e = 0; e < E; ++e)
+    for (int k = 0; k < 3; ++k)
+      if ((pl.edge[3 * (size_t)e + k].low & 3) == 3 && pl.wslot[e] < 0) {
+        pl.wslot[e] = (int)pl.welem.size();
+        pl.welem.push_back(e);
+      }
+  const int ns = (int)pl.welem.size();
+  std::vector<unsigned char> mask((size_t)ns * V, 0);
+  for (int s = 0; s < ns; ++s) {
+    const int e = pl.welem[s];
+    for (int k = 0; k < 3; ++k) {
+      const PlanEdge& ed = pl.edge[3 * (size_t)e + k];
+      if ((ed.low & 3) != 3) continue;
+      const int row = pl.rside[ed.bside];
+      for (int v = 0; v < V; ++v)
+        if (pl.rf_i[((size_t)row * V + v) * 2] >= 0) mask[(size_t)s * V + v] |= (1 << k) | (1 << ((k + 1) % 3));
+    }
+  }
+  pl.spec_par.clear();
+  pl.spec_seq.clear();
+  pl.spec_seq_off.assign(ns + 1, 0);
+  for (int s = 0; s < ns; ++s) {
+    const int e = pl.welem[s];
+    for (int v = 0; v < V; ++v) {
+      if (!mask[(size_t)s * V + v]) continue;
+      bool dep = false;
+      for (int k = 0; k < 3 && !dep; ++k) {
+        const PlanEdge& ed = pl.edge[3 * (size_t)e + k];
+        if ((ed.low & 3) != 3) continue;
+        const size_t o = ((size_t)pl.rside[ed.bside] * V + v) * 2;
+        if (pl.rf_i[o] < 0) continue;
+        for (int j = 0; j < 2 && !dep; ++j) {
+          const int I = pl.rf_i[o + j];
+          const unsigned char mI = mask[(size_t)s * V + I];
+          if (I < v && (((mI >> k) & 1) || ((mI >> ((k + 1) % 3)) & 1))) dep = true;
+        }
+      }
+      if (dep)
+        pl.spec_seq.push_back(s * V + v);
+      else
+        pl.spec_par.push_back(s * V + v);
+    }
+    pl.spec_seq_off[s + 1] = (int)pl.spec_seq.size();
+  }
+  pl.spec = true;
+  return 0;
+}
+
 int build_plan(const dgbgk_mesh& m, const dgbgk_vspace& vs, const dgbgk_params& p, int EB, Plan& pl,
                std::string* err) {
   auto fail = [&](int code, const std::string& msg) {
@@ -304,6 +435,15 @@ int build_plan(const dgbgk_mesh& m, const dgbgk_vspace& vs, const dgbgk_params& 
     w.any = m.rsido[3 * b + 1];
     w.sumbottom = sb;
     pl.walls.push_back(w);
+  }
+
+  // ---- the specular part of the wall flux for ALPHA < 1
+  pl.spec = false;
+  if (p.alpha != 1.0 && pl.has_wall_incoming) {
+    if (p.immat != 1)
+      return fail(DGBGK_EUNSUP, "dgbgk_create: wall accommodation ALPHA < 1 needs IMMAT = 1 in this build");
+    int rc = build_specular(m, vs, pl, err);
+    if (rc != 0) return rc;
   }
 
   // ---- Courant limit (src/alotim.f90:12-18, MXSPD = rv)

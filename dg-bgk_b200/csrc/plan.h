@@ -50,6 +50,24 @@ struct Plan {
   // nodal gather (MACROS tail / GETMAC): CSR over mesh nodes
   std::vector<int> node_off, node_dg;  // DG node index (plan order) per entry
   std::vector<double> node_ae;         // GEOME(7) of its element
+  // Wall accommodation ALPHA < 1 (IMMAT = 1): the specular part of GETBOU.
+  // A molecule leaving a wall side at velocity v (TEST < 0) carries
+  // (1-ALPHA) times the element's own f at the mirrored velocity, read as
+  // the two grid velocities I1, I2 around it and interpolated with ZD1, ZD2
+  // (src/getbou.f90:189-255).  The reference reads them from DISNF while its
+  // velocity loop updates it in place, so velocities I < v contribute their
+  // new values.  Items are (wall element slot, v) pairs with some node
+  // deferred; an item whose mirrored velocities include an earlier deferred
+  // one is "sequential" (processed per element in velocity order).
+  bool spec = false;
+  std::vector<int> welem;         // wall elements (plan order) by slot
+  std::vector<int> wslot;         // [E] slot of each element, -1 without a wall side
+  std::vector<int> rside;         // [B] reflection-table row of each wall side, -1 for others
+  std::vector<int> rf_i;          // [rows][V][2] I1, I2 (0-based); -1 where TEST >= 0
+  std::vector<double> rf_z;       // [rows][V][2] ZD1, ZD2
+  std::vector<int> spec_par;      // items slot*V + v processed in parallel
+  std::vector<int> spec_seq_off;  // [slots + 1]
+  std::vector<int> spec_seq;      // sequential items, per slot in velocity order
 };
 
 // Device edge word of edge i = 3*e + k (ElemEdge::info): the kind, the

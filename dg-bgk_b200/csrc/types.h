@@ -49,7 +49,8 @@ template <class T> struct alignas(16) ElemRec {
   ElemEdge<T> edge[3];
   int flags;  // bits [0,3): DG node i sits on an inflow-side node (INFLOW);
               // bits [3,6): edge k is a wall side
-  int pad1[3];
+  int wslot;  // wall element slot (ALPHA < 1: the deferred updates), else -1
+  int pad1[2];
 };
 static_assert(sizeof(ElemRec<float>) == 176 && sizeof(ElemRec<double>) == 336, "record layout");
 // values of the leading part a halo element needs (gx .. mu)

@@ -72,7 +72,7 @@ typedef struct dgbgk_vspace {
 typedef struct dgbgk_params {
   int immat;          /* 1: lumped mass (GETINC), 0: consistent (CMMINC)  */
   double csafm;       /* Courant safety factor                            */
-  double alpha;       /* wall accommodation (1 = fully diffuse)           */
+  double alpha;       /* wall accommodation (1 = fully diffuse; < 1 needs immat = 1) */
   double rgas;        /* gas constant R                                   */
   double molar_mass;  /* M                                                */
   double diameter;    /* molecular diameter d                             */

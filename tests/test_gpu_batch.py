@@ -85,3 +85,20 @@ def test_batch_cases_stop_on_their_own_tolerance():
     for c, n in zip(cases, steps):
         t = started(c, 64)
         assert t.advance(3000, tol=0.2)["steps"] == n
+
+
+def test_batch_with_partial_accommodation_equals_cases_alone():
+    # ALPHA = 0.9 cases (the specular part runs per case after the sweep)
+    # beside an ALPHA = 1 case
+    a = cavity_case(8, 12, 12, mach=0.3, kn=0.1)
+    a.alpha = 0.9
+    b = channel_case(-2.0, 4.0, -2.0, 2.0, 30, 20, 12, 12, mach=2.0, kn=0.05, obstacle_side=1.0)
+    b.alpha = 0.9
+    cases = [a, b, cavity_case(8, 8, 16, mach=0.3, kn=0.1)]
+    alone = [started(c, 64) for c in cases]
+    for s in alone:
+        s.advance(5)
+    batched = [started(c, 64) for c in cases]
+    Batch(batched, tune_steps=1).advance(5)
+    for s, t in zip(batched, alone):
+        assert rel_l2(s.get_state(), t.get_state()) <= 1e-13

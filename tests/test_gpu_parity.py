@@ -182,3 +182,60 @@ def test_odd_and_even_step_counts_continue_identically():
     t, _, _ = pair(small_channel())
     t.advance(7)
     np.testing.assert_array_equal(s.get_state(), t.get_state())
+
+
+# ---- partial wall accommodation (ALPHA < 1, the reference cases' 0.9) ----
+# GETBOU's specular part reads the element's own f at the mirrored velocity
+# in the reference's velocity order (new values for earlier velocities);
+# RORDER = TORDER, the grids the reference's ring lookup serves.  The cavity
+# has corner elements with two wall sides (chains of mirrored velocities).
+
+def cavity_alpha():
+    c = cavity_case(8, 12, 12, mach=0.3, kn=0.1)
+    c.alpha = 0.9
+    return c
+
+
+def channel_alpha():
+    c = channel_case(-2.0, 4.0, -2.0, 2.0, 30, 20, 12, 12, mach=2.0, kn=0.05, obstacle_side=1.0)
+    c.alpha = 0.9
+    return c
+
+
+@pytest.mark.parametrize("mk,steps", [(cavity_alpha, 1), (cavity_alpha, 10), (channel_alpha, 1), (channel_alpha, 10)])
+def test_partial_accommodation_matches_oracle(mk, steps):
+    s, o, f0 = pair(mk())
+    r = s.advance(steps)
+    q = o.advance(steps)
+    assert rel_l2(r["res_linf"], q["res_linf"]) <= 1e-9
+    assert rel_l2(r["res_l2"], q["res_l2"]) <= 1e-9
+    assert rel_l2(s.get_state(), o.get_state()) <= TOL64
+    compare_macros(s, o, TOL64)
+
+
+@pytest.mark.parametrize("mesh", ["tc3_nanotubesphere.plt.gz", "tc1_reentry.plt.gz"])
+def test_reference_meshes_partial_accommodation(mesh):
+    # the reference cases' own accommodation (ALPHA = 0.9, IMMAT = 1)
+    c = reference_case(load_plt(mesh), 10, 10, alpha=0.9, immat=1)
+    s, o, f0 = pair(c, lobatto=c.lobatto)
+    r = s.advance(2)
+    q = o.advance(2)
+    assert rel_l2(r["res_linf"], q["res_linf"]) <= 1e-9
+    assert rel_l2(s.get_state(), o.get_state()) <= TOL64
+    compare_macros(s, o, TOL64)
+
+
+def test_partial_accommodation_fp32_against_fp64_oracle():
+    s, o, f0 = pair(channel_alpha(), prec=32)
+    s.advance(5)
+    o.advance(5)
+    assert rel_l2(s.get_state(), o.get_state()) <= 1e-5
+
+
+def test_partial_accommodation_needs_lumped_mass():
+    from dgbgk._lib import DGBGK_EUNSUP, DgbgkError
+    c = cavity_alpha()
+    c.immat = 0
+    with pytest.raises(DgbgkError) as ei:
+        Solver.from_case(c, precision=64)
+    assert ei.value.code == DGBGK_EUNSUP

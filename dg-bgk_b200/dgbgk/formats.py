@@ -29,7 +29,7 @@ def write_lobatto(path, eta, w):
     with open(path, "w") as fh:
         fh.write(f"{len(eta)}\n")
         for a, b in zip(eta, w):
-            fh.write(f"{a!r}\t{b!r}\n")
+            fh.write(f"{float(a)!r}\t{float(b)!r}\n")
 
 
 def read_plt(path):
@@ -65,7 +65,8 @@ def write_plt(path, mesh, title="title"):
             fh.write(f"{i:10d}{a:15d}{b:10d}{c:10d}{0:10d}\n")
         fh.write("  coordinates \n")
         for i, (x, y) in enumerate(mesh.coord, 1):
-            fh.write(f"{i:10d}  {x: .15E}  {y: .15E}\n")
+            # 17 significant digits: the file holds the coordinates exactly
+            fh.write(f"{i:10d}  {x: .16E}  {y: .16E}\n")
         fh.write("  boundary sides \n")
         for r in mesh.bsido:
             fh.write("".join(f"{int(x):10d}" for x in r) + "\n")

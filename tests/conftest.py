@@ -26,4 +26,5 @@ def _make(d, target):
 def built_libraries():
     _make(ORACLE, os.path.join(ORACLE, "_build", "liboracle.so"))
     _make(PKG, os.path.join(PKG, "lib", "libdgbgk.so"))
+    _make(PKG, os.path.join(PKG, "bin", "dgbgk_run"))
     yield

@@ -1,0 +1,65 @@
+"""The command-line driver's namelist reader against the Python one (CPU).
+
+dgbgk_run --parse-only reads the &Input namelist the way the reference's
+driver does (quoted strings as gfortran writes them, bare ones as ifort
+accepts them, '!' comments, D exponents, the reference's defaults for what
+is left out) and prints it; no GPU is touched.
+"""
+import json
+import subprocess
+
+import pytest
+
+from cli_case import BIN, write_case
+from dgbgk import channel_case
+from dgbgk.formats import read_namelist
+
+
+@pytest.mark.parametrize("quoted", [True, False])
+def test_parse_only_matches_python_reader(tmp_path, quoted):
+    c = channel_case(-2.0, 4.0, -2.0, 2.0, 12, 8, 6, 6, mach=2.0, kn=0.05, obstacle_side=1.0)
+    c.alpha = 0.9
+    con = write_case(str(tmp_path), c, 1200, forceout=1, quoted=quoted)
+    got = json.loads(subprocess.run([BIN, con, "--parse-only"], capture_output=True, text=True, check=True).stdout)
+    ref = read_namelist(con)
+    for k, v in got.items():
+        if isinstance(v, list):
+            assert v == pytest.approx(ref[k], rel=1e-15)
+        elif isinstance(v, str):
+            assert v == ref[k]
+        else:
+            assert v == pytest.approx(ref[k], rel=1e-15), k
+    # defaults of the reference for keys the file leaves out
+    assert got["NVSPACEPART"] == 1 and got["W"] == 1.0
+
+
+def test_restart_input_is_refused(tmp_path):
+    c = channel_case(-2.0, 4.0, -2.0, 2.0, 12, 8, 6, 6, mach=2.0, kn=0.05, obstacle_side=1.0)
+    con = write_case(str(tmp_path), c, 10)
+    text = open(con).read().replace("IVD%RS = 0,", "IVD%RS = 1,")
+    open(con, "w").write(text)
+    r = subprocess.run([BIN, con], capture_output=True, text=True, cwd=str(tmp_path))
+    assert r.returncode != 0 and "restart" in r.stderr
+
+
+def test_lobatto_file_round_trip(tmp_path):
+    from dgbgk.cases import gll
+    from dgbgk.formats import read_lobatto, write_lobatto
+    eta, w = gll(12)
+    p = str(tmp_path / "lob.txt")
+    write_lobatto(p, eta, w)
+    n, e2, w2 = read_lobatto(p)
+    assert n == 12 and (e2 == eta).all() and (w2 == w).all()
+
+
+def test_plt_mesh_round_trip_is_exact(tmp_path):
+    # the driver's inputs hold the generated mesh bit for bit (the march
+    # amplifies last-digit changes of the geometry beyond the output format)
+    import numpy as np
+    from dgbgk.formats import read_plt, write_plt
+    c = channel_case(-5.0, 15.0, -10.0, 10.0, 40, 40, 4, 4, mach=2.0, kn=0.05, sides="freestream")
+    p = str(tmp_path / "m.plt")
+    write_plt(p, c.mesh)
+    m = read_plt(p)
+    assert np.array_equal(m.coord, c.mesh.coord) and np.array_equal(m.intma, c.mesh.intma)
+    assert np.array_equal(m.bsido, c.mesh.bsido)

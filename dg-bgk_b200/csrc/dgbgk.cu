@@ -86,6 +86,10 @@ struct ImplBase {
   // the state in the reference layout DISNF(3,VNPNT,NELEM), FP64, from / to
   // a device buffer (the stream is synchronised on return)
   virtual int export_device(double* buf) = 0;
+  // reduced-rank extrapolation: snapshot slots of the state (slot < 0 frees
+  // them), and the extrapolated state from slots 0 .. n-1
+  virtual int snapshot(int slot) = 0;
+  virtual int extrapolate(int n, double* gamma) = 0;
   virtual int import_device(const double* buf) = 0;
   Plan pl;
   int device = 0;
@@ -349,6 +353,10 @@ template <class T> struct Impl : ImplBase {
   int *rside = nullptr, *rf_i = nullptr, *welem = nullptr, *spec_par = nullptr, *spec_seq_off = nullptr,
       *spec_seq = nullptr;
   T *rf_z = nullptr, *wd = nullptr;
+  // extrapolation snapshots [snap_cap][3E*Vp] and the Gram / coefficient buffers
+  T* snaps = nullptr;
+  int snap_cap = 0;
+  double *d_gram = nullptr, *d_gamma = nullptr;
   CaseDev<T> hc;          // this case's table entry
   LaunchSet<T> single;    // this case alone
 
@@ -397,6 +405,9 @@ template <class T> struct Impl : ImplBase {
     dfree(spec_par);
     dfree(spec_seq_off);
     dfree(spec_seq);
+    dfree(snaps);
+    dfree(d_gram);
+    dfree(d_gamma);
     if (staging) cudaFree(staging);
     if (hctrl) cudaFreeHost(hctrl);
     if (ev0) cudaEventDestroy(ev0);
@@ -803,6 +814,97 @@ template <class T> struct Impl : ImplBase {
     cur = 0;
     return 0;
   }
+  int snapshot(int slot) override {
+    CK(cudaSetDevice(device));
+    const size_t N = (size_t)3 * pl.E * Vp;
+    if (slot < 0) {  // free the snapshots
+      CK(cudaStreamSynchronize(st));
+      dfree(snaps);
+      snap_cap = 0;
+      return 0;
+    }
+    if (slot >= RRE_MAX) {
+      set_error("dgbgk_snapshot: slot beyond the extrapolation limit of " + std::to_string(RRE_MAX) + " snapshots");
+      return DGBGK_EINVAL;
+    }
+    if (slot >= snap_cap) {  // grow, keeping the slots taken so far
+      T* nb = nullptr;
+      CK(cudaMalloc((void**)&nb, (size_t)(slot + 1) * N * sizeof(T)));
+      if (snaps) {
+        CK(cudaMemcpyAsync(nb, snaps, (size_t)snap_cap * N * sizeof(T), cudaMemcpyDeviceToDevice, st));
+        CK(cudaStreamSynchronize(st));
+        cudaFree(snaps);
+      }
+      snaps = nb;
+      snap_cap = slot + 1;
+    }
+    CK(cudaMemcpyAsync(snaps + (size_t)slot * N, f[cur], N * sizeof(T), cudaMemcpyDeviceToDevice, st));
+    CK(cudaStreamSynchronize(st));
+    return 0;
+  }
+  int extrapolate(int n, double* gamma) override {
+    CK(cudaSetDevice(device));
+    if (n < 2 || n > snap_cap) {
+      set_error("dgbgk_extrapolate: needs 2 <= n <= the snapshots taken");
+      return DGBGK_EINVAL;
+    }
+    const int m = n - 1;
+    const size_t N = (size_t)3 * pl.E * Vp;
+    if (!d_gram) TRY(dalloc(&d_gram, (size_t)RRE_MAX * RRE_MAX));
+    if (!d_gamma) TRY(dalloc(&d_gamma, (size_t)RRE_MAX));
+    CK(cudaMemsetAsync(d_gram, 0, (size_t)m * m * sizeof(double), st));
+    const int grid = (int)std::min<size_t>((size_t)4 * nsm, (N + 255) / 256);
+    k_gram<T><<<grid, 256, 0, st>>>(snaps, N, n, N, d_gram);
+    CK(cudaGetLastError());
+    std::vector<double> G((size_t)m * m);
+    CK(cudaMemcpyAsync(G.data(), d_gram, G.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    // G gamma = 1 (upper triangle accumulated), a tiny ridge, Gaussian
+    // elimination with partial pivoting, then sum(gamma) = 1
+    double tr = 0;
+    for (int a = 0; a < m; ++a) {
+      for (int b = 0; b < a; ++b) G[a * m + b] = G[b * m + a];
+      tr += G[a * m + a];
+    }
+    if (!(tr > 0) || !std::isfinite(tr)) {
+      set_error("dgbgk_extrapolate: the snapshots do not differ");
+      return DGBGK_EINVAL;
+    }
+    for (int a = 0; a < m; ++a) G[a * m + a] += 1e-14 * tr;
+    std::vector<double> g(m, 1.0);
+    for (int c = 0; c < m; ++c) {
+      int pv = c;
+      for (int r = c + 1; r < m; ++r)
+        if (std::fabs(G[r * m + c]) > std::fabs(G[pv * m + c])) pv = r;
+      if (pv != c) {
+        for (int k = 0; k < m; ++k) std::swap(G[c * m + k], G[pv * m + k]);
+        std::swap(g[c], g[pv]);
+      }
+      for (int r = c + 1; r < m; ++r) {
+        const double fct = G[r * m + c] / G[c * m + c];
+        for (int k = c; k < m; ++k) G[r * m + k] -= fct * G[c * m + k];
+        g[r] -= fct * g[c];
+      }
+    }
+    for (int c = m - 1; c >= 0; --c) {
+      for (int k = c + 1; k < m; ++k) g[c] -= G[c * m + k] * g[k];
+      g[c] /= G[c * m + c];
+    }
+    double sum = 0;
+    for (double x : g) sum += x;
+    for (auto& x : g) x /= sum;
+    for (double x : g)
+      if (!std::isfinite(x)) {
+        set_error("dgbgk_extrapolate: singular difference system");
+        return DGBGK_ENONFINITE;
+      }
+    if (gamma) std::copy(g.begin(), g.end(), gamma);
+    CK(cudaMemcpyAsync(d_gamma, g.data(), m * sizeof(double), cudaMemcpyHostToDevice, st));
+    k_combine<T><<<grid, 256, 0, st>>>(snaps, N, m, d_gamma, N, f[cur]);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(st));
+    return 0;
+  }
   int upload_perm() {
     if (d_inv) return 0;
     TRY(upload(&d_inv, pl.inv, st));
@@ -1103,6 +1205,14 @@ int dgbgk_get_residual_reference(dgbgk_handle* h, double* r) {
   if (!r) return set_error("NULL pointer"), DGBGK_EINVAL;
   *r = h->impl->ref_host;
   return 0;
+}
+int dgbgk_snapshot(dgbgk_handle* h, int slot) {
+  HCHECK(h);
+  return h->impl->snapshot(slot);
+}
+int dgbgk_extrapolate(dgbgk_handle* h, int n, double* gamma) {
+  HCHECK(h);
+  return h->impl->extrapolate(n, gamma);
 }
 int dgbgk_copy_state(dgbgk_handle* dst, const dgbgk_handle* src) {
   HCHECK(dst);

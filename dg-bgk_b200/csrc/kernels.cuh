@@ -1209,6 +1209,75 @@ __global__ void k_nodal(NodalArgs a) {
   a.temp[q] = t;
 }
 
+// ---------------------------------------------- vector extrapolation ----
+// Reduced-rank extrapolation of the pseudo-time iterates (no counterpart in
+// the reference; it changes the path to the fixed point, not the fixed
+// point): snapshots x_0 .. x_{n-1} of the state, differences
+// u_j = x_{j+1} - x_j.  k_gram accumulates G_ab = u_a . u_b (a <= b < n-1)
+// in FP64 (per-thread partials, a warp and block reduction, one atomic per
+// block and entry); k_combine writes max(sum_j gamma_j x_j, 0).
+constexpr int RRE_MAX = 11;  // snapshots (10 differences, 55 products)
+template <class T>
+__global__ void __launch_bounds__(256) k_gram(const T* __restrict__ snaps, size_t stride, int n, size_t N,
+                                              double* __restrict__ G) {
+  constexpr int MD = RRE_MAX - 1, NPAIR = MD * (MD + 1) / 2;
+  const int m = n - 1;
+  double acc[NPAIR];
+#pragma unroll
+  for (int q = 0; q < NPAIR; ++q) acc[q] = 0.0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < N; i += (size_t)gridDim.x * blockDim.x) {
+    double u[MD];
+    double prev = (double)snaps[i];
+#pragma unroll
+    for (int j = 0; j < MD; ++j) {
+      if (j < m) {
+        const double x = (double)snaps[(size_t)(j + 1) * stride + i];
+        u[j] = x - prev;
+        prev = x;
+      } else {
+        u[j] = 0.0;
+      }
+    }
+#pragma unroll
+    for (int a = 0; a < MD; ++a)
+#pragma unroll
+      for (int b = a; b < MD; ++b) {
+        const int q = a * MD - a * (a - 1) / 2 + (b - a);
+        acc[q] = fma(u[a], u[b], acc[q]);
+      }
+  }
+  __shared__ double red[8];
+#pragma unroll
+  for (int a = 0; a < MD; ++a)
+#pragma unroll
+    for (int b = a; b < MD; ++b) {
+      if (b >= m) continue;  // uniform over the block
+      const int q = a * MD - a * (a - 1) / 2 + (b - a);
+      const double v = warp_sum(acc[q]);
+      if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+        atomicAdd(&G[a * m + b], t);
+      }
+      __syncthreads();
+    }
+}
+
+template <class T>
+__global__ void __launch_bounds__(256) k_combine(const T* __restrict__ snaps, size_t stride, int m,
+                                                 const double* __restrict__ gamma, size_t N, T* __restrict__ out) {
+  __shared__ double g[RRE_MAX];
+  if (threadIdx.x < RRE_MAX) g[threadIdx.x] = (int)threadIdx.x < m ? gamma[threadIdx.x] : 0.0;
+  __syncthreads();
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < N; i += (size_t)gridDim.x * blockDim.x) {
+    double x = 0.0;
+    for (int j = 0; j < m; ++j) x = fma(g[j], (double)snaps[(size_t)j * stride + i], x);
+    out[i] = (T)(x > 0.0 ? x : 0.0);
+  }
+}
+
 // ----------------------------------------------------- layout changes ----
 // reference DISNF(3,V,E) (old element order) <-> f rows (plan order, pitch Vp)
 template <class S, class T>

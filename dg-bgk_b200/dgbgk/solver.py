@@ -209,6 +209,16 @@ class Solver:
         check(lib().dgbgk_get_residual_reference(self.h, ctypes.byref(r)))
         return r.value
 
+    def snapshot(self, slot):
+        """Copies the state into extrapolation slot `slot` (< 0: frees them)."""
+        check(lib().dgbgk_snapshot(self.h, slot))
+
+    def extrapolate(self, n):
+        """Reduced-rank extrapolation from slots 0 .. n-1; returns gamma."""
+        g = np.zeros(max(n - 1, 1))
+        check(lib().dgbgk_extrapolate(self.h, n, ptr(g)))
+        return g[:n - 1]
+
     def copy_state_from(self, other):
         """Takes `other`'s state (converted to this handle's precision on the
         device) and residual reference; same mesh and velocity grid."""

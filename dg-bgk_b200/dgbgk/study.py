@@ -19,6 +19,8 @@ start) four ways:
                then the state is handed to FP64 handles (dgbgk_copy_state)
                and the batch finishes to 1e-8
   fast_cold    as fast, from the cold start (no network)
+  *_rre        the same with reduced-rank extrapolation of the iterates
+               (march_batch_rre: the same fixed point in fewer steps)
 
 A stored FP32 state stops changing once every update is below half an ulp,
 so an FP32 march settles anywhere within about tau * ulp / 2 of its fixed
@@ -149,6 +151,71 @@ def march_batch(b, solvers, tol, max_steps, chunk=1000, stall=0.8, stall_below=1
     return steps, rel, status, dev
 
 
+def march_batch_rre(b, solvers, tol, max_steps, start=1e-2, every=100, m=8, stall=0.8, stall_below=1e-3):
+    """march_batch with reduced-rank extrapolation (dgbgk_extrapolate):
+    once a case's relative residual is below `start`, each cycle of `every`
+    steps ends with m + 1 single steps whose m + 2 states the case
+    snapshots and extrapolates from.  A case whose residual grew tenfold
+    over the cycle after an extrapolation extrapolates no more.  The fixed
+    point and the convergence test are the march's own; only the path to it
+    changes."""
+    from ._lib import DgbgkError
+    n = len(solvers)
+    steps = np.zeros(n, dtype=np.int64)
+    status = np.zeros(n, dtype=np.int32)
+    prev = np.full(n, np.inf)
+    rel = np.full(n, np.inf)
+    done = np.zeros(n, dtype=bool)
+    use = np.ones(n, dtype=bool)
+    dev = [0.0]
+    refs = np.array([s.residual_reference() for s in solvers])
+
+    def adv(k):
+        r = b.advance(k, tol=tol, raise_on_error=False)
+        dev[0] += b.last_ms() * 1e-3
+        live = (status == 0) & ~done
+        steps[live] += r["steps"][live]
+        status[live] = r["status"][live]
+        now = r["res_l2_last"] / np.maximum(refs, 1e-300)
+        rel[:] = np.where(live & (r["steps"] > 0), now, rel)
+        done[:] |= (status != 0) | (rel <= tol * (1 + 1e-9))
+
+    cyc_before = np.full(n, np.inf)
+    win_start = 0  # the stall test compares residuals 1000 steps apart
+    while steps.max() < max_steps and not done.all():
+        adv(every - (m + 1))
+        grew = use & np.isfinite(cyc_before) & (rel > 10 * cyc_before)
+        use &= ~grew
+        if steps.max() - win_start >= 1000:
+            stalled = (rel > stall * prev) & (rel < stall_below) & ~done
+            prev = rel.copy()
+            win_start = int(steps.max())
+            done |= stalled
+        if done.all():
+            break
+        act = np.flatnonzero(~done & use & (rel < start))
+        cyc_before[:] = np.inf
+        if len(act) == 0:
+            continue
+        for i in act:
+            solvers[i].snapshot(0)
+        for j in range(m + 1):
+            adv(1)
+            for i in act:
+                solvers[i].snapshot(j + 1)
+        for i in act:
+            if done[i]:
+                continue
+            cyc_before[i] = rel[i]
+            try:
+                solvers[i].extrapolate(m + 2)
+            except DgbgkError:
+                use[i] = False
+    for s in solvers:
+        s.snapshot(-1)
+    return steps, rel.copy(), status, dev[0]
+
+
 def generate(cases, precision=32, tol=1e-5, accept=1e-4, group=64, max_steps=60000, log=None):
     """Marches the cases (batches of `group`) to tol, or to their FP32
     rounding plateau; keeps those whose relative residual is <= accept.
@@ -269,7 +336,7 @@ def evaluate(cases, ws, tol=1e-8, switch_tol=1e-5, max_steps=200000,
         if log:
             log(f"plain: {wall:.2f} s, steps {min(steps)}..{max(steps)}, dropped {out['dropped']}")
 
-    def batched(name, warm, precision_first, switch):
+    def batched(name, warm, precision_first, switch, rre=False):
         t0 = time.perf_counter()
         first = [Solver.from_case(c, precision=precision_first, device=device) for c in cases]
         fin = [Solver.from_case(c, precision=64, device=device) for c in cases] if switch else first
@@ -285,7 +352,10 @@ def evaluate(cases, ws, tol=1e-8, switch_tol=1e-5, max_steps=200000,
         t_init = time.perf_counter() - t
         b = Batch(first)
         t_tune = time.perf_counter() - t
-        if switch:
+        if rre:
+            steps1, _, st1, dev = march_batch_rre(b, first, switch or tol, max_steps,
+                                                  stall_below=1e-3 if switch else 0.0)
+        elif switch:
             steps1, _, st1, dev = march_batch(b, first, switch, max_steps)
         else:
             steps1, _, st1, dev = march_batch(b, first, tol, max_steps, chunk=max_steps, stall_below=0.0)
@@ -310,9 +380,13 @@ def evaluate(cases, ws, tol=1e-8, switch_tol=1e-5, max_steps=200000,
             for a, s in zip(fin, first):
                 a.copy_state_from(s)
             b2 = Batch(fin)
-            r2 = b2.advance(max_steps, tol=tol)
-            dev += b2.last_ms() * 1e-3
-            steps2 = r2["steps"]
+            if rre:
+                steps2, _, _, d2 = march_batch_rre(b2, fin, tol, max_steps, stall_below=0.0)
+                dev += d2
+            else:
+                r2 = b2.advance(max_steps, tol=tol)
+                dev += b2.last_ms() * 1e-3
+                steps2 = r2["steps"]
             b2.close()
         wall = time.perf_counter() - t
         fields = [nodal_fields(s, c) for s, c in zip(fin, cases)]
@@ -336,6 +410,12 @@ def evaluate(cases, ws, tol=1e-8, switch_tol=1e-5, max_steps=200000,
         out["fast"] = batched("fast", True, 32, switch_tol)
     if "fast_cold" in ways:
         out["fast_cold"] = batched("fast_cold", False, 32, switch_tol)
+    if "batch64_rre" in ways:
+        out["batch64_rre"] = batched("batch64_rre", False, 64, None, rre=True)
+    if "fast_rre" in ways:
+        out["fast_rre"] = batched("fast_rre", True, 32, switch_tol, rre=True)
+    if "fast_cold_rre" in ways:
+        out["fast_cold_rre"] = batched("fast_cold_rre", False, 32, switch_tol, rre=True)
     if "plain" in final:
         for k in final:
             if k == "plain":

@@ -153,6 +153,19 @@ int dgbgk_get_residual_reference(dgbgk_handle* h, double* res_l2_ref);
  * be on one device and built from the same mesh and velocity grid. */
 int dgbgk_copy_state(dgbgk_handle* dst, const dgbgk_handle* src);
 
+/* No counterpart in the reference.  Reduced-rank extrapolation of the
+ * pseudo-time iterates, a way to reach the same fixed point in fewer steps:
+ * dgbgk_snapshot copies the current state into slot (0 <= slot < 11; the
+ * slots are allocated on the device as they are first used; slot < 0 frees
+ * them).  dgbgk_extrapolate takes the snapshots x_0 .. x_{n-1} of
+ * consecutive iterates, finds gamma (n-1 values, sum 1) minimising
+ * |sum_j gamma_j (x_{j+1} - x_j)|, and replaces the state by
+ * max(sum_j gamma_j x_j, 0); gamma (may be NULL) receives the coefficients.
+ * The march goes on from there: its residual test decides convergence as
+ * before. */
+int dgbgk_snapshot(dgbgk_handle* h, int slot);
+int dgbgk_extrapolate(dgbgk_handle* h, int n, double* gamma);
+
 /* MACROS (src/macros.f90:51-188) + GETMAC (src/getmac.f90:98-123) of the
  * current state: nodal ND, RHO, UVEL, VVEL, PS, TEMP, NPOIN values each. */
 int dgbgk_get_macros(dgbgk_handle* h, double* nd, double* rho, double* u, double* v, double* ps,

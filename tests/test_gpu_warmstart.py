@@ -114,3 +114,49 @@ def test_trained_network_gains_over_the_cold_start():
     assert max(e["n"], e["u"], e["T"]) <= 1e-6
     plain.close()
     warm.close()
+
+
+def test_extrapolation_matches_numpy_rre():
+    # dgbgk_extrapolate on five consecutive iterates: the coefficients and
+    # the extrapolated state equal a float64 restatement of reduced-rank
+    # extrapolation on the same snapshots
+    c = family_case(2.5, 0.07)
+    s, _ = cold(c, 64, 0.0, max_steps=40)
+    xs = []
+    for j in range(5):
+        s.snapshot(j)
+        xs.append(s.get_state())
+        if j < 4:
+            s.advance(1)
+    g = s.extrapolate(5)
+    U = np.stack([(xs[j + 1] - xs[j]).ravel() for j in range(4)])
+    G = U @ U.T
+    G += 1e-14 * np.trace(G) * np.eye(4)
+    gr = np.linalg.solve(G, np.ones(4))
+    gr /= gr.sum()
+    # the difference system is ill-conditioned (coefficients of opposite
+    # signs and |gamma| >> 1): summation order moves gamma at ~1e-7
+    np.testing.assert_allclose(g, gr, rtol=1e-4)
+    x = np.maximum(sum(gj * xj for gj, xj in zip(g, xs[:4])), 0.0)
+    assert rel_l2(s.get_state(), x) <= 1e-12
+    s.snapshot(-1)
+    s.close()
+
+
+def test_extrapolated_march_reaches_the_same_fixed_point_sooner():
+    from dgbgk.study import march_batch_rre
+    c = family_case(2.5, 0.07)
+    ref = cold_reference(c)
+    plain, r = cold(c, 64, 1e-8, ref)
+    s = Solver.from_case(c, precision=64)
+    s.init_case()
+    s.set_residual_reference(ref)
+    b = Batch([s], tune_steps=1)
+    steps, rel, status, _ = march_batch_rre(b, [s], 1e-8, 60000, stall_below=0.0)
+    assert status[0] == 0 and rel[0] <= 1e-8 * (1 + 1e-9)
+    assert steps[0] < 0.8 * r["steps"], (steps[0], r["steps"])
+    e = rel_fields(nodal_fields(s, c), nodal_fields(plain, c))
+    assert max(e["n"], e["u"], e["T"]) <= 1e-6
+    b.close()
+    plain.close()
+    s.close()

@@ -1,6 +1,6 @@
 // dgbgk_run: the reference's driver on the sm_100a library, one partition.
 //
-//   dgbgk_run case.con [--precision 64|32] [--device N] [--tol X] [--parse-only]
+//   dgbgk_run case.con [--precision 64|32] [--device N] [--tol X] [--restart-out] [--parse-only]
 //
 // Follows src/spectralbgk.f90 (the &Input namelist with its defaults, the
 // Lobatto file, the .plt mesh and the FILE.OUT echo), DG_LIN_CONVEC's setup
@@ -10,11 +10,17 @@
 // RESIDUAL.RES line per step (log of max|DELUN| over the first step's, with
 // GETFOR's lift and drag when FORCEOUT != 0, src/getfor.f90).  Files are
 // opened by the names the namelist gives, relative to the working directory,
-// as the reference does.  Restart input (RS = 1) is not read.
+// as the reference does.  RS = 1 starts from RestartInFile in the format
+// INICON2 reads (src/inicon2.f90:61-114): a title line, NPOIN and VNPNT,
+// then one line per velocity and element (velocity outer) whose first
+// three values are DISNF(1:3, IV, IE).
 //
 // Extensions: --precision 32 stores f in FP32; --tol stops when the L2
-// residual falls to tol times the first step's; --parse-only prints the
-// parsed inputs as JSON and exits (no GPU needed).
+// residual falls to tol times the first step's; --restart-out writes the
+// final state to RestartOutFile in the format RS = 1 reads (the reference's
+// own writer, src/output.f90, is not called by its driver and writes a
+// layout its reader does not take); --parse-only prints the parsed inputs as
+// JSON and exits (no GPU needed).
 #include <cctype>
 #include <cmath>
 #include <cstdio>
@@ -268,7 +274,7 @@ int main(int argc, char** argv) {
   std::string con;
   int precision = 64, device = 0;
   double tol = 0.0;
-  bool parse_only = false;
+  bool parse_only = false, restart_out = false;
   for (int i = 1; i < argc; ++i) {
     std::string a = argv[i];
     if (a == "--precision" && i + 1 < argc)
@@ -279,12 +285,15 @@ int main(int argc, char** argv) {
       tol = std::atof(argv[++i]);
     else if (a == "--parse-only")
       parse_only = true;
+    else if (a == "--restart-out")
+      restart_out = true;
     else if (con.empty())
       con = a;
     else
       return die("unexpected argument " + a);
   }
-  if (con.empty()) return die("usage: dgbgk_run case.con [--precision 64|32] [--device N] [--tol X] [--parse-only]");
+  if (con.empty())
+    return die("usage: dgbgk_run case.con [--precision 64|32] [--device N] [--tol X] [--restart-out] [--parse-only]");
   Input in;
   std::string err;
   if (!parse_con(con, in, err)) return die(err);
@@ -300,7 +309,6 @@ int main(int argc, char** argv) {
                 in.ResultsFile1.c_str(), in.ResultsFile2.c_str());
     return 0;
   }
-  if (in.RS == 1) return die("restart input (RS = 1) is not supported by this driver");
 
   // velocity space (src/spectralbgk.f90:156-161, src/vspace.f90)
   std::vector<double> eta, wl;
@@ -322,6 +330,40 @@ int main(int argc, char** argv) {
     std::fprintf(fo, "LOBATTO ORDER      TOTAL NUMBER OF NODES\n");
     std::fprintf(fo, "%6d%6d%6d\n", RORDER, TORDER, V);
     std::fclose(fo);
+  }
+
+  // INICON2's restart input, read (and checked) before any device work
+  std::vector<double> disnf0;
+  if (in.RS == 1) {
+    disnf0.assign(3 * (size_t)V * m.nelem, 0.0);
+    // INICON2's restart branch (src/inicon2.f90:61-114)
+    std::ifstream rf(in.RestartInFile);
+    if (!rf) return die("cannot open the restart file " + in.RestartInFile);
+    std::string l1, l2;
+    std::getline(rf, l1);
+    std::getline(rf, l2);
+    long long t1 = -1, t2 = -1;
+    {
+      std::istringstream is(l2);
+      is >> t1 >> t2;
+    }
+    if (t1 != m.npoin || t2 != V) return die("THIS RESTART FILE IS NOT COMPATIBLE WITH YOUR MESHES!");
+    std::string line;
+    for (int iv = 0; iv < V; ++iv)
+      for (int ie = 0; ie < m.nelem; ++ie) {
+        // list-directed READ of three values: the first three of the record
+        int got = 0;
+        double vals[3];
+        while (got < 3 && std::getline(rf, line)) {
+          for (auto& c : line)
+            if (c == 'd' || c == 'D') c = 'e';
+          std::istringstream is(line);
+          double x;
+          while (got < 3 && (is >> x)) vals[got++] = x;
+        }
+        if (got < 3) return die("truncated restart file " + in.RestartInFile);
+        for (int k = 0; k < 3; ++k) disnf0[(size_t)k + 3 * ((size_t)iv + (size_t)V * ie)] = vals[k];
+      }
   }
 
   // setup (src/dg_lin_convec.f90:70-89)
@@ -351,8 +393,12 @@ int main(int argc, char** argv) {
   p.device = device;
   dgbgk_handle* h = nullptr;
   if (dgbgk_create(&dm, &vs, &p, &h) != 0) return die(dgbgk_last_error());
-  // INICON2 (src/inicon2.f90:120-182)
-  if (dgbgk_init_uniform(h, in.T1, in.P1, in.U0, in.V0, nullptr) != 0) return die(dgbgk_last_error());
+  if (in.RS == 1) {
+    if (dgbgk_set_state(h, disnf0.data()) != 0) return die(dgbgk_last_error());
+  } else {
+    // INICON2 (src/inicon2.f90:120-182)
+    if (dgbgk_init_uniform(h, in.T1, in.P1, in.U0, in.V0, nullptr) != 0) return die(dgbgk_last_error());
+  }
 
   FILE* f16 = std::fopen(in.ResidualFile.c_str(), "w");
   FILE* f17 = std::fopen(in.ResultsFile1.c_str(), "w");
@@ -414,6 +460,19 @@ int main(int argc, char** argv) {
   std::fclose(f16);
   std::fclose(f17);
   std::fclose(f18);
+  if (restart_out) {
+    std::vector<double> disnf(3 * (size_t)V * m.nelem);
+    if (dgbgk_get_state(h, disnf.data()) != 0) return die(dgbgk_last_error());
+    FILE* fr = std::fopen(in.RestartOutFile.c_str(), "w");
+    if (!fr) return die("cannot write " + in.RestartOutFile);
+    std::fprintf(fr, "NPOIN     VNPNT\n%12d    %12d\n", m.npoin, V);
+    for (int iv = 0; iv < V; ++iv)
+      for (int ie = 0; ie < m.nelem; ++ie) {
+        const double* q = &disnf[3 * ((size_t)iv + (size_t)V * ie)];
+        std::fprintf(fr, "%.17E %.17E %.17E\n", q[0], q[1], q[2]);
+      }
+    std::fclose(fr);
+  }
   std::printf("dgbgk_run: %d steps of %d elements x %d velocities (FP%d)%s\n", itime, m.nelem, V, precision,
               stopped ? ", stopped at the L2 tolerance" : "");
   dgbgk_destroy(h);

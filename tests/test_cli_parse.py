@@ -33,13 +33,16 @@ def test_parse_only_matches_python_reader(tmp_path, quoted):
     assert got["NVSPACEPART"] == 1 and got["W"] == 1.0
 
 
-def test_restart_input_is_refused(tmp_path):
+def test_incompatible_restart_file_is_refused(tmp_path):
+    # the check of INICON2's restart branch: NPOIN and VNPNT must match (it
+    # comes before any device work)
     c = channel_case(-2.0, 4.0, -2.0, 2.0, 12, 8, 6, 6, mach=2.0, kn=0.05, obstacle_side=1.0)
     con = write_case(str(tmp_path), c, 10)
-    text = open(con).read().replace("IVD%RS = 0,", "IVD%RS = 1,")
+    text = open(con).read().replace("IVD%RS = 0,", 'IVD%RS = 1,\nIVD%RestartInFile = "old.res",')
     open(con, "w").write(text)
+    open(str(tmp_path / "old.res"), "w").write("NPOIN     VNPNT\n 7 36\n")
     r = subprocess.run([BIN, con], capture_output=True, text=True, cwd=str(tmp_path))
-    assert r.returncode != 0 and "restart" in r.stderr
+    assert r.returncode != 0 and "NOT COMPATIBLE" in r.stderr
 
 
 def test_lobatto_file_round_trip(tmp_path):

@@ -83,3 +83,26 @@ def test_driver_matches_library(tmp_path):
     out = open(os.path.join(d, "FILE.OUT")).read().splitlines()
     assert out[-1] == f"{20:6d}{20:6d}{400:6d}" and out[-3] == "V-SPACE STATS:"
     s.close()
+
+
+def test_restart_round_trip_continues_exactly(tmp_path):
+    # 10 steps, write the restart file, read it back (RS = 1) for 10 more:
+    # the state equals 20 steps in one run (the file holds 17 digits)
+    c = channel_case(-5.0, 15.0, -10.0, 10.0, 100, 100, 20, 20, mach=2.5, kn=0.07, obstacle_side=1.0,
+                     sides="freestream")
+    c.alpha = 0.9
+    d1, d2 = str(tmp_path / "a"), str(tmp_path / "b")
+    os.makedirs(d1)
+    os.makedirs(d2)
+    one = write_case(d1, c, 20)
+    assert subprocess.run([BIN, one, "--restart-out"], capture_output=True, cwd=d1).returncode == 0
+    first = write_case(d2, c, 10)
+    assert subprocess.run([BIN, first, "--restart-out"], capture_output=True, cwd=d2).returncode == 0
+    os.replace(os.path.join(d2, "RESTART.RES"), os.path.join(d2, "half.res"))
+    text = open(first).read().replace("IVD%RS = 0,", 'IVD%RS = 1,\nIVD%RestartInFile = "half.res",')
+    open(first, "w").write(text)
+    r = subprocess.run([BIN, first, "--restart-out"], capture_output=True, text=True, cwd=d2)
+    assert r.returncode == 0, r.stderr
+    a = open(os.path.join(d1, "RESTART.RES")).read()
+    b = open(os.path.join(d2, "RESTART.RES")).read()
+    assert a == b

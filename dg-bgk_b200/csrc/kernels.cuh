@@ -940,7 +940,10 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : 1)
             }
             // GETINC / CMMINC, ADTHEM (f >= 0), INFLOW; the padding past V
             // stays zero
-            auto finish = [&](auto full) {
+            // defer: some node of this chunk waits for the specular part
+            // (only wall elements with ALPHA < 1; the other variant has no
+            // per-value test)
+            auto finish = [&](auto full, auto defer) {
 #pragma unroll
               for (int w = 0; w < W; ++w) {
                 const bool live = decltype(full)::value || vb + w < C.V;
@@ -965,7 +968,7 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : 1)
                   const T ch = (fn < (T)0) ? -f : d;
                   fn = fn > (T)0 ? fn : (T)0;
                   if (live) {
-                    if ((dmask >> (3 * w + i)) & 1u) {
+                    if (decltype(defer)::value && ((dmask >> (3 * w + i)) & 1u)) {
                       // deferred: k_wspec adds the specular part, clips and
                       // counts the residual
                       C.wd[((size_t)r.wslot * 3 + i) * C.Vp + vb + w] = d;
@@ -980,10 +983,17 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : 1)
                 }
               }
             };
-            if (vb + W <= C.V)
-              finish(std::true_type());
-            else
-              finish(std::false_type());
+            if (dmask != 0u) {
+              if (vb + W <= C.V)
+                finish(std::true_type(), std::true_type());
+              else
+                finish(std::false_type(), std::true_type());
+            } else {
+              if (vb + W <= C.V)
+                finish(std::true_type(), std::false_type());
+              else
+                finish(std::false_type(), std::false_type());
+            }
             if (flags & 7) {
               const VecT nf = vld<T>(vn + cq * W);  // zero past V
 #pragma unroll

@@ -281,19 +281,21 @@ def run_ours(a, d):
         out["fp32_over_fp64_per_step"] = out["value"] / out["fp64"]["value"]
         del s64
     # time to steady state (L2 residual 1e-8 of a cold start's first step)
-    # on eight channels of the warm-start family, three ways: plain FP64 one
-    # case at a time; FP64 in one batch; FP32 in one batch until 1e-5 (or
-    # its rounding plateau), then FP64 to 1e-8 (the precision handoff).  The
-    # network's share is measured by dgbgk.study (results/).
+    # on eight channels of the warm-start family: plain FP64 one case at a
+    # time; FP64 in one batch; FP32 in one batch until 1e-5 (or its rounding
+    # plateau), then FP64 to 1e-8 (the precision handoff); the same with
+    # reduced-rank extrapolation of the iterates.  The network's share is
+    # measured by dgbgk.study (results/).
     if not a.no_steady and d.world == 1:
         from dgbgk.study import draw_cases, evaluate
         cases = draw_cases(8, 77)
-        res, _, kept = evaluate(cases, None, ways=("plain", "batch64", "fast_cold"), device=d.local)
+        res, _, kept = evaluate(cases, None, ways=("plain", "batch64", "fast_cold", "fast_cold_rre"),
+                                device=d.local)
         st = {"cases": f"{len(kept)} channels [-5,15]x[-10,10], 100x100 quads, 16x32 velocities, free-stream "
                        "sides, Mach/Kn/obstacle drawn (dgbgk.study.draw_cases(8, 77))",
               "dofs_per_case": kept[0].dofs if kept else 0, "tol": 1e-8, "switch_tol": res["switch_tol"],
               "plain_fp64_s": res["plain"]["wall_s"], "plain_fp64_steps": int(sum(res["plain"]["steps"]))}
-        for k in ("batch64", "fast_cold"):
+        for k in ("batch64", "fast_cold", "fast_cold_rre"):
             st[k] = {"wall_s": res[k]["wall_s"], "speedup_vs_plain": res[k]["speedup_vs_plain"],
                      "steps": int(sum(res[k]["steps"])), "steps_fp64_finish": int(sum(res[k]["steps_fp64_finish"])),
                      "max_rel_l2_vs_plain": res[k]["max_rel_l2_vs_plain"]}

@@ -7,7 +7,9 @@ supersonic channel: [-5,15]x[-5,5] as 200x100 quads (39 800 P1 triangles)
 minus a unit-square obstacle, 24 x 48 velocities (1.3755e8 DOFs), Mach 2,
 Kn 0.05, f stored in FP32 with FP64 moments and residual norms.  The metric
 is DOF-updates/s = 3*NELEM*VNPNT*steps / device time of the time loop.
-Beside it (one GPU): the plain FP64 path on the same workload, the time to
+Beside it (one GPU): the reference's own test case tc1 timed per step (its
+one published timing is 0.123 s per step on 160 MPI ranks), the plain FP64
+path on the same workload, the time to
 steady state (L2 residual 1e-8) of eight warm-start-family channels plain
 FP64 vs batched FP64 vs batched FP32 with an FP64 finish, the end-to-end
 rate through the C ABI with host buffers, and the oracle on the host cores.
@@ -50,6 +52,7 @@ def args():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-steady", action="store_true", help="skip the time-to-steady-state leg")
+    ap.add_argument("--no-tc1", action="store_true", help="skip the reference test case tc1 leg")
     return ap.parse_args()
 
 
@@ -215,6 +218,45 @@ def oracle_step_rate(case, nsteps, threads, warmup=0, min_seconds=0.0):
     return case.dofs * nsteps / dt, dt, nsteps
 
 
+# The reference's own test case tc1 (tc/tc1/reentry_test.con: 28 304 P1
+# elements, Lobatto40 x 40 angles = 1.359e8 DOFs, ALPHA 0.9, IMMAT 1, the
+# namelist's gas with the reference's defaults R 287, M 32, d 250e-12),
+# built from the committed fixtures, and the one published timing of the
+# reference: 0.123 s per pseudo-time step on 160 MPI ranks, FP32
+# (tc/tc1/output over its 2000 steps).
+TC1_PUBLISHED_S_PER_STEP = 0.123
+
+
+def tc1_leg(device, steps=40, warmup=3):
+    from dgbgk.formats import read_lobatto, read_plt
+    from dgbgk.solver import Solver, setup_mesh, vspace
+    g = os.path.join(ROOT, "tests", "golden")
+    mesh = read_plt(os.path.join(g, "tc1_reentry.plt.gz"))
+    n, eta, w = read_lobatto(os.path.join(g, "Lobatto40.txt"))
+    nml = json.load(open(os.path.join(g, "kat.json")))["tc1_namelist"]
+    f = lambda k: float(nml[k])
+    to = int(nml["TORDER"])
+    st = setup_mesh(mesh.intma, mesh.coord, mesh.bsido)
+    vc, sw = vspace(n, to, eta, w)
+    dofs = 3 * mesh.nelem * n * to
+    out = {"case": f"tc1 reentry: {mesh.nelem} P1 elements x {n}x{to} velocities = {dofs} DOFs, ALPHA "
+                   f"{nml['ALPHA']}, IMMAT {nml['IMMAT']}", "dofs": dofs,
+           "published_reference_s_per_step": TC1_PUBLISHED_S_PER_STEP,
+           "published_reference_setup": "160 MPI ranks (16 space x 10 velocity partitions), FP32"}
+    for prec in (32, 64):
+        s = Solver(mesh.intma, mesh.coord, mesh.bsido, st, vc, sw, n, to, f("rv"), immat=int(nml["IMMAT"]),
+                   csafm=f("CSAFM"), alpha=f("ALPHA"), rgas=287.0, molar_mass=32.0, diameter=250e-12,
+                   cinf=(f("CINF(1)"), f("CINF(2)"), f("CINF(3)"), f("CINF(4)")), precision=prec, device=device)
+        s.inicon2(f("T1"), f("P1"), f("U0"), f("V0"))
+        s.advance(warmup)
+        s.advance(steps)
+        ms = s.last_ms() / steps
+        out[f"fp{prec}"] = {"ms_per_step": ms, "dof_updates_per_s": dofs / (ms * 1e-3),
+                            "speedup_vs_published": TC1_PUBLISHED_S_PER_STEP / (ms * 1e-3)}
+        del s
+    return out
+
+
 # ------------------------------------------------------------- our arm ----
 def run_ours(a, d):
     import numpy as np
@@ -300,6 +342,8 @@ def run_ours(a, d):
                      "steps": int(sum(res[k]["steps"])), "steps_fp64_finish": int(sum(res[k]["steps_fp64_finish"])),
                      "max_rel_l2_vs_plain": res[k]["max_rel_l2_vs_plain"]}
         out["steady_state"] = st
+    if not a.no_tc1 and d.world == 1:
+        out["reference_case_tc1"] = tc1_leg(d.local)
     # end to end through the C ABI with host buffers
     if not a.no_e2e:
         s = Solver.from_case(case, precision=a.precision, device=d.local)

@@ -33,8 +33,14 @@ def write_lobatto(path, eta, w):
 
 
 def read_plt(path):
-    with open(path) as fh:
-        lines = fh.read().splitlines()
+    """The .plt mesh; a path ending in .gz is read through gzip."""
+    if str(path).endswith(".gz"):
+        import gzip
+        with gzip.open(path, "rt") as fh:
+            lines = fh.read().splitlines()
+    else:
+        with open(path) as fh:
+            lines = fh.read().splitlines()
     pos = 0
     nlines = int(lines[pos].split()[0]); pos += 1
     pos += nlines          # title lines

@@ -1,0 +1,89 @@
+"""The host-side march drivers of the warm-start study on a fake batch (CPU).
+
+A fake case's residual follows a prescribed sequence per step; the drivers
+must stop a case at its tolerance, at its FP32 rounding plateau (the
+residual fell by less than 20% over 1000 steps below 1e-3) or when it
+diverges, and the extrapolating driver must snapshot m + 2 iterates per
+cycle, extrapolate only below `start`, and give up on a case whose
+residual grew tenfold after an extrapolation.
+"""
+import numpy as np
+
+from dgbgk._lib import DGBGK_ENONFINITE
+from dgbgk.study import march_batch, march_batch_rre
+
+
+class FakeCase:
+    def __init__(self, res, ref=1.0):
+        self.res = res          # function: step -> relative residual (nan: diverged)
+        self.step = 0
+        self.ref = ref
+        self.snaps = []
+        self.extrapolations = 0
+        self.jump = None        # after an extrapolation, add this to the step count
+
+    def residual_reference(self):
+        return self.ref
+
+    def snapshot(self, slot):
+        if slot >= 0:
+            self.snaps.append(slot)
+
+    def extrapolate(self, n):
+        assert n == len(self.snaps[-n:]) and self.snaps[-n:] == list(range(n))
+        self.extrapolations += 1
+        if self.jump:
+            self.step += self.jump
+        return np.ones(n - 1) / (n - 1)
+
+
+class FakeBatch:
+    def __init__(self, cases):
+        self.cases = cases
+
+    def advance(self, k, tol=0.0, raise_on_error=False):
+        steps, last, status = [], [], []
+        for c in self.cases:
+            n, r, st = 0, np.inf, 0
+            for _ in range(k):
+                c.step += 1
+                n += 1
+                r = c.res(c.step)
+                if not np.isfinite(r):
+                    st = DGBGK_ENONFINITE
+                    break
+                if tol > 0 and r <= tol:
+                    break
+            steps.append(n)
+            last.append(r * c.ref)
+            status.append(st)
+        return {"steps": np.array(steps), "res_l2_last": np.array(last), "status": np.array(status, dtype=np.int32)}
+
+    def last_ms(self):
+        return 0.0
+
+
+def test_march_batch_stops_at_tolerance_plateau_and_divergence():
+    fast = FakeCase(lambda k: 10 ** (-k / 500))                    # reaches 1e-8 at step 4000
+    plateau = FakeCase(lambda k: max(10 ** (-k / 500), 2e-6))      # FP32 rounding plateau
+    bad = FakeCase(lambda k: np.nan if k > 1500 else 1.0)
+    cases = [fast, plateau, bad]
+    steps, rel, status, _ = march_batch(FakeBatch(cases), cases, 1e-8, 60000)
+    assert steps[0] == 4000 and rel[0] <= 1e-8
+    assert status[1] == 0 and abs(rel[1] - 2e-6) < 1e-12 and steps[1] < 6000
+    assert status[2] == DGBGK_ENONFINITE
+
+
+def test_rre_driver_cycles_and_guard():
+    good = FakeCase(lambda k: 10 ** (-k / 1000))
+    good.jump = 300                     # an extrapolation skips 300 steps of decay
+    worse = FakeCase(lambda k: 10 ** (-k / 1000) * (20.0 if worse.extrapolations else 1.0))
+    cases = [good, worse]
+    steps, rel, status, _ = march_batch_rre(FakeBatch(cases), cases, 1e-8, 60000, stall_below=0.0)
+    assert rel[0] <= 1e-8 and good.extrapolations > 3
+    # no extrapolation above start = 1e-2 (residual 1e-2 at step 2000)
+    assert steps[0] < 8000
+    # the case whose residual grew tenfold after its first extrapolation stops extrapolating
+    assert worse.extrapolations == 1 and rel[1] <= 1e-8
+    # m + 2 = 10 snapshots per cycle
+    assert len(good.snaps) == 10 * good.extrapolations

@@ -173,9 +173,12 @@ inline int tiles_per_unit(long total_tiles, int grid0, int upc, int nvt) {
 
 // Uploads the case table and picks the launch shapes.  Moments: per-warp
 // rings of R-row stages; picks (R, warps per CTA, ring stages) with the most
-// resident warps per SM, then the most rows in flight, then the fewest rows
-// per warp step (measured on B200 at 24x48 velocities: one row per warp step
-// was fastest in FP32 and FP64).
+// resident warps per SM (shared memory and registers), then the most rows in
+// flight, then the fewest rows per warp step.  Measured on B200 at 24x48
+// velocities: one row per warp step was fastest in FP32 and FP64; warps
+// count for more than stages (FP64: 20 warps with one-stage rings 0.344 ms,
+// 16 with one 0.372, 10 with two 0.486; FP32: 20 with one 0.204, 16 with
+// two 0.207).
 template <class T>
 int build_launch_set(LaunchSet<T>& L, const std::vector<CaseDev<T>>& cs, int eb, int immat, int max_halo, int nsm,
                      cudaStream_t st, int force_rows = 0) {
@@ -188,15 +191,21 @@ int build_launch_set(LaunchSet<T>& L, const std::vector<CaseDev<T>>& cs, int eb,
   for (const auto& c : cs) maxrow = std::max(maxrow, c.rowbytes);
   // one case: its moment tables sit in shared memory
   const size_t tbytes = one ? (3 * (size_t)cs[0].Vp * sizeof(T) + 127) / 128 * 128 : 0;
-  const size_t cap = 227 * 1024, sm_total = 228 * 1024;
+  const size_t cap = 227 * 1024;
   long best = -1;
   for (int R : {4, 2, 1})
-    for (int w : {16, 12, 10, 8, 6, 5, 4, 3, 2, 1})
-      for (int sg : {3, 2}) {
+    for (int w : {20, 16, 12, 10, 8, 6, 5, 4, 3, 2, 1})
+      for (int sg : {3, 2, 1}) {
         if (force_rows > 0 && R != force_rows) continue;
+        if (w > 16 && !one) continue;  // 640 threads: the single-case kernel only
         const size_t bytes = 128 * (((size_t)w * sg * 8 + 127) / 128) + tbytes + (size_t)w * sg * R * maxrow;
         if (bytes > cap) continue;
-        const int blocks = (int)std::min<size_t>(4, sm_total / (bytes + 1024));
+        // resident CTAs per SM (shared memory and registers)
+        const void* mfn = (const void*)mom_fn<T>(R, one);
+        int blocks = 0;
+        TRY(allow_max_smem(mfn));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, mfn, w * 32, bytes));
+        blocks = std::min(blocks, 4);
         if (blocks < 1) continue;
         const long score = ((long)blocks * w * 1024 + (long)blocks * w * (sg - 1) * R) * 8 + (8 - R);
         if (score > best) {
@@ -286,8 +295,8 @@ template <class T> int enqueue_step(const LaunchSet<T>& L, cudaStream_t st, floa
   TRY(launch_check("k_moments", L.mom_grid, L.mom_warps * 32, L.mom_smem));
   if (ms) cudaEventRecord(ev[1], st);
   if (L.total_walls > 0) {
-    k_wall<T><<<(L.total_walls + 7) / 8, 256, 0, st>>>(L.args, L.total_walls);
-    TRY(launch_check("k_wall", (L.total_walls + 7) / 8, 256, 0));
+    k_wall<T><<<L.total_walls, WALL_THREADS, 0, st>>>(L.args, L.total_walls);
+    TRY(launch_check("k_wall", L.total_walls, WALL_THREADS, 0));
   }
   if (ms) cudaEventRecord(ev[2], st);
   constexpr int TPE = SweepGeo<T>::TPE;
@@ -418,7 +427,10 @@ template <class T> struct Impl : ImplBase {
   }
 
   int nvt() const { return (pl.V + SweepGeo<T>::VT - 1) / SweepGeo<T>::VT; }
-  static int default_eb() { return 128; }
+  // measured on B200 (channel 200x100, 24x48 velocities): FP32 sweep 0.414 ms
+  // at 128 elements per tile, 0.50 at 64; FP64 1.28 ms at 128 (one CTA of
+  // 8 warps per SM), 1.17 at 64 (three CTAs of 4 warps)
+  static int default_eb() { return sizeof(T) == 8 ? 64 : 128; }
 
   int init(int tile_elems) {
     CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
@@ -1068,7 +1080,7 @@ template <class T> struct Impl : ImplBase {
     TRY(aux_ctrl());
     CK(cudaMemsetAsync(bEtaD, 0, std::max(pl.B, 1) * sizeof(double), st));
     if (single.total_walls > 0) {
-      k_wall<T><<<(single.total_walls + 7) / 8, 256, 0, st>>>(single.args, single.total_walls);
+      k_wall<T><<<single.total_walls, WALL_THREADS, 0, st>>>(single.args, single.total_walls);
       CK(cudaGetLastError());
     }
     if (pl.B) CK(cudaMemcpyAsync(eta, bEtaD, pl.B * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -1137,7 +1149,9 @@ int dgbgk_create(const dgbgk_mesh* mesh, const dgbgk_vspace* vs, const dgbgk_par
   impl->device = prm->device;
   impl->prec = prm->precision;
   std::string err;
-  const int eb0 = prm->tile_elems > 0 ? prm->tile_elems : 128;
+  const int eb0 = prm->tile_elems > 0      ? prm->tile_elems
+                  : prm->precision == 64 ? Impl<double>::default_eb()
+                                         : Impl<float>::default_eb();
   int rc = build_plan(*mesh, *vs, *prm, eb0, impl->pl, &err);
   if (rc != 0) {
     set_error(err);

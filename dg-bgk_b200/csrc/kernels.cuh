@@ -296,9 +296,10 @@ template <int L> __device__ __forceinline__ double group_sum(double v) {
 // as a kernel parameter, with its velocity tables staged in shared memory;
 // otherwise the case table, with the tables read through L1 (they differ
 // from case to case).  MU's maximum goes to the case's control block once
-// per warp and case.
+// per warp and case.  Up to 20 warps per CTA for a single case (at
+// most 96 registers), 16 for the case table.
 template <class T, int R, bool ONE>
-__global__ void __launch_bounds__(512, 1)
+__global__ void __launch_bounds__(ONE ? 640 : 512, 1)
     k_moments(BatchArgs<T> a, int total_groups, const __grid_constant__ CaseDev<T> one) {
   constexpr int L = 32 / R;
   extern __shared__ __align__(128) unsigned char sm_raw[];
@@ -432,25 +433,35 @@ __global__ void __launch_bounds__(512, 1)
 }
 
 // --------------------------------------------------------- wall flux ----
-// FLUCON2 (src/flucon2.f90:134-233): one warp per wall side of any case.
-template <class T> __global__ void __launch_bounds__(256) k_wall(BatchArgs<T> a, int total_walls) {
-  const int w = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+// FLUCON2 (src/flucon2.f90:134-233): one CTA (WALL_THREADS threads) per
+// wall side of any case, its threads strided over the velocities, then a
+// block sum (a warp per side left the loads of a side in a serial chain:
+// ~37 us on the 200x100 channel's 40 wall sides).
+constexpr int WALL_THREADS = 256;
+template <class T> __global__ void __launch_bounds__(WALL_THREADS) k_wall(BatchArgs<T> a, int total_walls) {
+  __shared__ double part[WALL_THREADS / 32];
+  const int w = blockIdx.x, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (w >= total_walls) return;
   const int c = find_case(a.wall_off, a.ncases, w);
   const CaseDev<T>& C = a.cases[c];
-  if (C.ctrl->done) return;
+  if (C.ctrl->done) return;  // the same for the whole CTA
   const WallSide ws = C.walls[w - a.wall_off[c]];
   const T* f = C.f[C.ctrl->cur];
   const T* f1 = f + ((size_t)ws.elem * 3 + ws.in1) * C.Vp;
   const T* f2 = f + ((size_t)ws.elem * 3 + ws.in2) * C.Vp;
   double s = 0;
-  for (int v = lane; v < C.V; v += 32) {
+  for (int v = threadIdx.x; v < C.V; v += WALL_THREADS) {
     const double test = C.cxD[v] * ws.anx + C.cyD[v] * ws.any;
     if (test > 0.0) s += fabs(test) * (0.5 * ((double)f1[v] + (double)f2[v])) * C.wjf[v];
   }
   s = warp_sum(s);
-  if (lane == 0) {
-    const double eta = s / ws.sumbottom;
+  if (lane == 0) part[warp] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+#pragma unroll
+    for (int k = 0; k < WALL_THREADS / 32; ++k) t += part[k];
+    const double eta = t / ws.sumbottom;
     C.bEtaD[ws.bside] = eta;
     C.bEta[ws.bside] = (T)eta;
   }
@@ -656,8 +667,12 @@ __device__ __forceinline__ void sweep_p1(const ElemRec<T>& r, unsigned char* tl,
 // Upwinding: the own value is taken where SC = n.c > 0.  The reference takes
 // it where SC > 0 for the ISIDE(3) element and SC >= 0 for the other; the
 // two differ only at SC = 0, where the flux SC*value is zero either way.
+// Residency: FP32, two CTAs per SM (128 registers); FP64 with 64-element
+// blocks, three CTAs of 4 warps (168 registers, a few spilled: 1.17 ms per
+// sweep on the 200x100 channel at 24x48 velocities, against 1.28 ms for one
+// 8-warp CTA of 128 elements at 228 registers).
 template <class T, int EB, int IMMAT, bool ONE>
-__global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : 1)
+__global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : (EB == 64 ? 3 : 1))
     k_sweep(BatchArgs<T> a, int total_units, const __grid_constant__ CaseDev<T> one) {
   using G = SweepGeo<T>;
   using VO = Vec<T>;

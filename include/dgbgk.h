@@ -82,7 +82,7 @@ typedef struct dgbgk_params {
                          in FP32 with FP64 moments and residual norms      */
   const double* wall_velocity; /* (2,NBOUN) moving-wall velocity per
                                   boundary side, or NULL (all at rest)    */
-  int tile_elems;     /* sweep tile: elements per CTA (0 = default)        */
+  int tile_elems;     /* sweep tile: elements per CTA, 64 or 128 (0: 128 for FP32, 64 for FP64) */
   int tile_vels;      /* sweep tile: velocities per CTA (0 = default)      */
   int device;         /* CUDA device ordinal                               */
 } dgbgk_params;

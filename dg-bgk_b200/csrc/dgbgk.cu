@@ -428,8 +428,8 @@ template <class T> struct Impl : ImplBase {
 
   int nvt() const { return (pl.V + SweepGeo<T>::VT - 1) / SweepGeo<T>::VT; }
   // measured on B200 (channel 200x100, 24x48 velocities): FP32 sweep 0.414 ms
-  // at 128 elements per tile, 0.50 at 64; FP64 1.28 ms at 128 (one CTA of
-  // 8 warps per SM), 1.17 at 64 (three CTAs of 4 warps)
+  // at 128 elements per tile, 0.50 at 64; FP64 1.24 ms at 128 (one CTA of
+  // 8 warps per SM), 1.02 at 64 (three CTAs of 4 warps)
   static int default_eb() { return sizeof(T) == 8 ? 64 : 128; }
 
   int init(int tile_elems) {

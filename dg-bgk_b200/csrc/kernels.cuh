@@ -29,6 +29,7 @@
 
 #include <type_traits>
 
+#include "exp_tang.h"
 #include "types.h"
 
 namespace dgbgk {
@@ -556,12 +557,15 @@ template <int N> __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-// exp of the NFO exponent: FP64 exp(x); FP32 2^x from the SFU (ex2.approx,
-// relative error ~2^-22; the FP32 coefficient carries the log2(e) factor,
-// applied in FP64 by the moment kernel).
-template <class T> __device__ __forceinline__ T nfo_exp(T x);
-template <> __device__ __forceinline__ double nfo_exp<double>(double x) { return exp(x); }
-template <> __device__ __forceinline__ float nfo_exp<float>(float x) {
+// exp of the NFO exponent: FP64 by Tang's table-driven method (exp_tang.h,
+// about one ulp, `tab` the CTA's 2^(j/64) table); FP32 2^x from the SFU
+// (ex2.approx, relative error ~2^-22; the FP32 coefficient carries the
+// log2(e) factor, applied in FP64 by the moment kernel; no table).
+template <class T> __device__ __forceinline__ T nfo_exp(T x, const double* tab);
+template <> __device__ __forceinline__ double nfo_exp<double>(double x, const double* tab) {
+  return exp_tang(x, tab);
+}
+template <> __device__ __forceinline__ float nfo_exp<float>(float x, const double*) {
   float p;
   asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(p) : "f"(x));
   return p;
@@ -609,7 +613,7 @@ template <class T> __device__ __forceinline__ void vst(void* p, const typename V
 // volume term of this element use (src/getelc.f90:87-117,
 // src/edgflxopt.f90:95-125); NFO and UMEAN are returned.
 template <class T>
-__device__ __forceinline__ void sweep_p1(const ElemRec<T>& r, unsigned char* tl, int r0, int c,
+__device__ __forceinline__ void sweep_p1(const ElemRec<T>& r, const double* etab, unsigned char* tl, int r0, int c,
                                          const typename Vec<T>::type& cxv, const typename Vec<T>::type& cyv, T dth,
                                          T dth3, typename Vec<T>::type (&q)[3], typename Vec<T>::type& u) {
   using VO = Vec<T>;
@@ -631,7 +635,7 @@ __device__ __forceinline__ void sweep_p1(const ElemRec<T>& r, unsigned char* tl,
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
       const T dx = r.ux[i] - cx, dy = r.uy[i] - cy;
-      const T qi = r.A[i] * nfo_exp<T>(r.ex[i] * (dx * dx + dy * dy));
+      const T qi = r.A[i] * nfo_exp<T>(r.ex[i] * (dx * dx + dy * dy), etab);
       VO::set(q[i], w, qi);
       coll += r.mu[i] * (qi - VO::get(f[i], w));
     }
@@ -668,9 +672,9 @@ __device__ __forceinline__ void sweep_p1(const ElemRec<T>& r, unsigned char* tl,
 // it where SC > 0 for the ISIDE(3) element and SC >= 0 for the other; the
 // two differ only at SC = 0, where the flux SC*value is zero either way.
 // Residency: FP32, two CTAs per SM (128 registers); FP64 with 64-element
-// blocks, three CTAs of 4 warps (168 registers, a few spilled: 1.17 ms per
-// sweep on the 200x100 channel at 24x48 velocities, against 1.28 ms for one
-// 8-warp CTA of 128 elements at 228 registers).
+// blocks, three CTAs of 4 warps (168 registers, a few spilled: 1.02 ms per
+// sweep on the 200x100 channel at 24x48 velocities, against 1.24 ms for one
+// 8-warp CTA of 128 elements at 208 registers).
 template <class T, int EB, int IMMAT, bool ONE>
 __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : (EB == 64 ? 3 : 1))
     k_sweep(BatchArgs<T> a, int total_units, const __grid_constant__ CaseDev<T> one) {
@@ -687,7 +691,11 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : (E
   __shared__ int s_unit;
   __shared__ double red_m[NW], red_s[NW];
   __shared__ uint64_t bars[2];  // TMA completion of tile buffer 0 / 1
+  // FP64: the 2^(j/64) table of the NFO exp (one entry for FP32, unused)
+  __shared__ double etab[sizeof(T) == 8 ? EXP_TAB : 1];
   const int tid = threadIdx.x;
+  if (sizeof(T) == 8)
+    for (int i = tid; i < EXP_TAB; i += NT) etab[i] = exp2((double)i / EXP_TAB);
   // tile buffers 1024-byte aligned (the swizzle pattern repeats every 512 B)
   unsigned char* const base = sm_raw + ((1024u - (smem_u32(sm_raw) & 1023u)) & 1023u);
   const size_t tile_bytes = G::tile_bytes(EB, a.max_halo);
@@ -811,14 +819,14 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : (E
 #pragma unroll
           for (int cc = 0; cc < CPT; ++cc) {
             const int cq = CPT * hh + cc;
-            sweep_p1<T>(r, tl, 3 * j, cq, vld<T>(vx + cq * W), vld<T>(vy + cq * W), dth, dth3, qr[cc], ur[cc]);
+            sweep_p1<T>(r, etab, tl, 3 * j, cq, vld<T>(vx + cq * W), vld<T>(vy + cq * W), dth, dth3, qr[cc], ur[cc]);
           }
         }
         for (int w = tid; w < nh * NCH; w += NT) {
           const int hs = w >> 2, cq = w & 3;
           const ElemRec<T>& r = *reinterpret_cast<const ElemRec<T>*>(hrec + (size_t)hs * HR);
           VecT qd[3], ud;
-          sweep_p1<T>(r, tl, 3 * (EB + hs), cq, vld<T>(vx + cq * W), vld<T>(vy + cq * W), dth, dth3, qd, ud);
+          sweep_p1<T>(r, etab, tl, 3 * (EB + hs), cq, vld<T>(vx + cq * W), vld<T>(vy + cq * W), dth, dth3, qd, ud);
         }
         __syncthreads();
         // the other buffer's tile k - 1 is stored (or being stored): load tile k + 1

@@ -4,7 +4,7 @@ and what the trained network gains over a cold start.
 The cases are the warm-start family's channel (free-stream sides, 100 x 100
 quads) on a 12 x 24 velocity grid, drawn from the middle of the family's
 ranges, so that a test marches in seconds (an 8 x 16 grid is too coarse: the
-explicit scheme diverges on it).  The cold FP64 march is the judge: a
+explicit scheme diverges on it).  The cold FP64 march is the yardstick: a
 warm-started (or FP32-started) march must end, at the same residual, on the
 same fields.
 """

@@ -2,6 +2,11 @@
 steady state with and without it.
 
     python -m dgbgk.study --train 384 --test 32 --out study.json
+    torchrun --nproc-per-node 8 --master-addr 127.0.0.1 -m dgbgk.study ...
+
+Under torchrun the training set is generated by every rank, each on its own
+GPU, as a round-robin share of the cases (independent steady states: no
+data crosses GPUs), and gathered once by rank 0, which trains and evaluates.
 
 A family of supersonic channel cases (square obstacle; Mach, Kn and the
 obstacle side drawn per case) is marched to steady state by the batch API
@@ -32,6 +37,7 @@ fields are compared with the plain path's.
 import argparse
 import json
 import math
+import os
 import time
 
 import numpy as np
@@ -216,21 +222,33 @@ def march_batch_rre(b, solvers, tol, max_steps, start=1e-2, every=100, m=8, stal
     return steps, rel.copy(), status, dev[0]
 
 
-def generate(cases, precision=32, tol=1e-5, accept=1e-4, group=64, max_steps=60000, log=None):
-    """Marches the cases (batches of `group`) to tol, or to their FP32
-    rounding plateau; keeps those whose relative residual is <= accept.
-    Returns X (n, 3), Y (n, 4 * 64 * 128) and the kept case indices."""
+def shard(n, rank, world):
+    """The case indices one rank of `world` generates: rank, rank + world, ...
+    (round robin, so every rank gets the same mix of mesh sizes and Mach
+    numbers).  The cases are independent steady states: no data crosses
+    ranks until the finished sets are gathered."""
+    return list(range(rank, n, world))
+
+
+def generate(cases, precision=32, tol=1e-5, accept=1e-4, group=64, max_steps=60000, log=None, rank=0, world=1,
+             device=0):
+    """Marches this rank's share of the cases (batches of `group`) to tol, or
+    to their FP32 rounding plateau; keeps those whose relative residual is
+    <= accept.  Returns X (n, 3), Y (n, 4 * 64 * 128) and the kept cases'
+    indices into `cases`."""
     X, Y, keep = [], [], []
-    for g0 in range(0, len(cases), group):
-        part = cases[g0:g0 + group]
-        ss = [Solver.from_case(c, precision=precision) for c in part]
+    idx = shard(len(cases), rank, world)
+    for g0 in range(0, len(idx), group):
+        part_idx = idx[g0:g0 + group]
+        part = [cases[i] for i in part_idx]
+        ss = [Solver.from_case(c, precision=precision, device=device) for c in part]
         for s in ss:
             s.init_case()
         b = Batch(ss)
         t = time.perf_counter()
         steps, rel, status, dev = march_batch(b, ss, tol, max_steps)
         if log:
-            log(f"generate {g0}..{g0 + len(part)}: steps {int(steps.min())}..{int(steps.max())} "
+            log(f"generate rank {rank}/{world} {g0}..{g0 + len(part)}: steps {int(steps.min())}..{int(steps.max())} "
                 f"diverged {int((status != 0).sum())} kept {int(((status == 0) & (rel <= accept)).sum())} "
                 f"device {dev:.1f} s wall {time.perf_counter() - t:.1f} s")
         for k, (c, s) in enumerate(zip(part, ss)):
@@ -238,11 +256,23 @@ def generate(cases, precision=32, tol=1e-5, accept=1e-4, group=64, max_steps=600
                 q = nodal_fields(s, c)
                 X.append(params_vector(c))
                 Y.append(resampler(c).to_grid(q).reshape(-1).astype(np.float32))
-                keep.append(g0 + k)
+                keep.append(part_idx[k])
         b.close()
         for s in ss:
             s.close()
     return np.array(X, dtype=np.float32), np.array(Y, dtype=np.float32), keep
+
+
+def merge_generated(parts):
+    """The (X, Y, keep) sets of every rank as one set in case order."""
+    parts = [p for p in parts if len(p[2])]
+    if not parts:
+        return np.zeros((0, 3), np.float32), np.zeros((0, NF * GRID[0] * GRID[1]), np.float32), []
+    X = np.concatenate([p[0] for p in parts])
+    Y = np.concatenate([p[1] for p in parts])
+    keep = [i for p in parts for i in p[2]]
+    order = np.argsort(keep, kind="stable")
+    return X[order], Y[order], [keep[i] for i in order]
 
 
 class WarmStart:
@@ -443,14 +473,34 @@ def main(argv=None):
     ap.add_argument("--switch-tol", type=float, default=1e-5)
     ap.add_argument("--ways", default="plain,batch64,batch64_warm,fast")
     ap.add_argument("--out", default=None)
+    ap.add_argument("--gather-timeout", type=float, default=7200.0,
+                    help="seconds a rank may wait for the others' training sets (torchrun)")
     a = ap.parse_args(argv)
 
     def log(m):
         print(m, flush=True)
 
+    # torchrun: every rank generates its share of the training set on its own
+    # GPU; rank 0 gathers the sets (host objects over gloo, once, with a
+    # timeout above a share's generation time), trains and evaluates
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=a.gather_timeout))
     t = time.perf_counter()
     train_cases = draw_cases(a.train, a.seed)
-    X, Y, keep = generate(train_cases, tol=a.data_tol, log=log)
+    X, Y, keep = generate(train_cases, tol=a.data_tol, log=log, rank=rank, world=world, device=local)
+    if dist is not None:
+        parts = [None] * world if rank == 0 else None
+        dist.gather_object((X, Y, keep), parts, dst=0)
+        dist.destroy_process_group()
+        if rank != 0:
+            return
+        X, Y, keep = merge_generated(parts)
     gen_s = time.perf_counter() - t
     log(f"training set: {len(keep)} of {a.train} cases kept ({gen_s:.1f} s)")
     ws = WarmStart()

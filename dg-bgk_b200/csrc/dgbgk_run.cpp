@@ -126,8 +126,14 @@ bool parse_con(const std::string& path, Input& in, std::string& err) {
   return true;
 }
 
-// Fortran 1PE12.5
+// Fortran 1PE12.5 (a non-finite value is written as gfortran writes it,
+// right-aligned NaN / Infinity)
 std::string fe12(double x) {
+  if (!std::isfinite(x)) {
+    std::string r = std::isnan(x) ? "NaN" : (x > 0 ? "Infinity" : "-Infinity");
+    while (r.size() < 12) r = " " + r;
+    return r;
+  }
   char buf[64];
   std::snprintf(buf, sizeof buf, "%.5E", x);
   std::string s(buf);
@@ -194,6 +200,7 @@ bool read_plt(const std::string& path, Mesh& m, std::string& err) {
     std::istringstream is(line);
     is >> m.nelem >> m.npoin >> m.nboun;
   }
+  if (m.nelem <= 0 || m.npoin <= 0 || m.nboun < 0) return err = "bad element / point / boundary counts", false;
   char b18[64];
   std::snprintf(b18, sizeof b18, "%6d%6d%6d", m.nelem, m.npoin, m.nboun);
   m.echo.push_back(b18);
@@ -230,7 +237,9 @@ bool read_lobatto(const std::string& path, std::vector<double>& eta, std::vector
   if (!fh) return err = "cannot open the Lobatto file " + path, false;
   std::string tok;
   fh >> tok;
-  const int n = (int)std::lround(std::strtod(tok.c_str(), nullptr));
+  const double nd = std::strtod(tok.c_str(), nullptr);
+  if (!(nd >= 1.0 && nd <= 1.0e6)) return err = "bad point count in the Lobatto file " + path, false;
+  const int n = (int)std::lround(nd);
   eta.resize(n);
   w.resize(n);
   for (int i = 0; i < n; ++i) {

@@ -66,3 +66,32 @@ def test_plt_mesh_round_trip_is_exact(tmp_path):
     m = read_plt(p)
     assert np.array_equal(m.coord, c.mesh.coord) and np.array_equal(m.intma, c.mesh.intma)
     assert np.array_equal(m.bsido, c.mesh.bsido)
+
+
+@pytest.mark.parametrize("damage,message", [
+    ("lobatto_count", "bad point count in the Lobatto file"),
+    ("lobatto_short", "truncated Lobatto file"),
+    ("mesh_counts", "bad element / point / boundary counts"),
+    ("mesh_short", "truncated"),
+])
+def test_malformed_inputs_are_refused(tmp_path, damage, message):
+    # broken input files end the driver with a message before any device
+    # work (the velocity space and the mesh are read and set up on the host)
+    c = channel_case(-2.0, 4.0, -2.0, 2.0, 12, 8, 6, 6, mach=2.0, kn=0.05, obstacle_side=1.0)
+    con = write_case(str(tmp_path), c, 10)
+    lob, mesh = tmp_path / "lob.txt", tmp_path / "mesh.plt"
+    if damage == "lobatto_count":
+        lines = lob.read_text().splitlines()
+        lob.write_text("\n".join(["-3"] + lines[1:]) + "\n")
+    elif damage == "lobatto_short":
+        lob.write_text("\n".join(lob.read_text().splitlines()[:3]) + "\n")
+    elif damage == "mesh_counts":
+        text = mesh.read_text().splitlines()
+        k = next(i for i, ln in enumerate(text) if ln.split()[:3] == [str(c.mesh.nelem), str(c.mesh.npoin),
+                                                                      str(c.mesh.nboun)])
+        text[k] = f"-{c.mesh.nelem} {c.mesh.npoin} {c.mesh.nboun}"
+        mesh.write_text("\n".join(text) + "\n")
+    else:
+        mesh.write_text("\n".join(mesh.read_text().splitlines()[:40]) + "\n")
+    r = subprocess.run([BIN, con], capture_output=True, text=True, cwd=str(tmp_path), timeout=60)
+    assert r.returncode != 0 and message in r.stderr, (r.returncode, r.stderr[-500:])

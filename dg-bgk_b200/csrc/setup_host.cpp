@@ -167,6 +167,11 @@ extern "C" int dgbgk_setup_mesh(int nelem, int npoin, int nboun, const int* intm
     double dx = coord[2 * (r.b - 1)] - coord[2 * (r.a - 1)];
     double dy = coord[2 * (r.b - 1) + 1] - coord[2 * (r.a - 1) + 1];
     double L = std::sqrt((dx * dx) + (dy * dy));
+    if (!(L > 0.0) || !std::isfinite(L)) {  // the reference would divide by zero here
+      dgbgk::set_error("dgbgk_setup_mesh: side between nodes " + std::to_string(r.a) + " and " +
+                       std::to_string(r.b) + " has zero or non-finite length");
+      return DGBGK_EMESH;
+    }
     el[s] = L;
     nx[s] = dy / L;
     ny[s] = -dx / L;
@@ -182,6 +187,10 @@ extern "C" int dgbgk_setup_mesh(int nelem, int npoin, int nboun, const int* intm
     }
     double x21 = X[1] - X[0], x31 = X[2] - X[0], y21 = Y[1] - Y[0], y31 = Y[2] - Y[0];
     double rj = x21 * y31 - x31 * y21;
+    if (!(rj != 0.0) || !std::isfinite(rj)) {
+      dgbgk::set_error("dgbgk_setup_mesh: element " + std::to_string(e + 1) + " has zero or non-finite area");
+      return DGBGK_EMESH;
+    }
     double rj1 = 1. / rj;
     double xix = y31 * rj1, xiy = -x31 * rj1, etx = -y21 * rj1, ety = x21 * rj1;
     double* G = &geome[7 * e];
@@ -212,6 +221,10 @@ extern "C" int dgbgk_setup_mesh(int nelem, int npoin, int nboun, const int* intm
     double dx = coord[2 * (p1 - 1)] - coord[2 * (p0 - 1)];
     double dy = coord[2 * (p1 - 1) + 1] - coord[2 * (p0 - 1) + 1];
     double rl = std::sqrt(dx * dx + dy * dy);
+    if (!(rl > 0.0)) {
+      dgbgk::set_error("dgbgk_setup_mesh: boundary side " + std::to_string(b + 1) + " has zero length");
+      return DGBGK_EMESH;
+    }
     double rt = 1.0 / rl;
     rsido[3 * b] = dy * rt;
     rsido[3 * b + 1] = -dx * rt;

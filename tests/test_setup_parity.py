@@ -59,3 +59,35 @@ def test_boundary_conventions_of_generated_meshes():
         for b, row in enumerate(m.bsido):
             mid = 0.5 * (m.coord[row[0] - 1] + m.coord[row[1] - 1])
             assert np.dot(st.rsido[b, :2], mid - cen[row[2] - 1]) > 0
+
+
+@pytest.mark.parametrize("damage,code,message", [
+    ("node_index", -2, "INTMA references a node outside"),
+    ("bside_index", -2, "BSIDO references a node outside"),
+    ("zero_area", -2, "has zero or non-finite area"),
+    ("zero_side", -2, "has zero or non-finite length"),
+    ("no_elements", -1, "bad arguments"),
+])
+def test_setup_refuses_broken_meshes(damage, code, message):
+    # broken meshes end with a status code and a message (the reference
+    # would divide by zero or index out of bounds); host only, no GPU
+    from dgbgk._lib import DgbgkError
+    m = cavity_mesh(4, 0.3)
+    intma, coord, bsido = m.intma.copy(), m.coord.copy(), m.bsido.copy()
+    if damage == "node_index":
+        intma[5, 1] = m.npoin + 1
+    elif damage == "bside_index":
+        bsido[2, 0] = 0
+    elif damage == "zero_area":
+        # element 1's three nodes on one line: its third node moved onto
+        # the line through the first two
+        a, b, c = intma[0] - 1
+        coord[c] = 0.5 * (coord[a] + coord[b])
+    elif damage == "zero_side":
+        a, b, _ = intma[0] - 1
+        coord[b] = coord[a]
+    else:
+        intma = intma[:0]
+    with pytest.raises(DgbgkError) as ei:
+        setup_mesh(intma, coord, bsido)
+    assert ei.value.code == code and message in str(ei.value)

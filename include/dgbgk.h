@@ -31,7 +31,7 @@ extern "C" {
 
 #define DGBGK_OK 0
 #define DGBGK_EINVAL (-1)    /* bad size, pointer or parameter */
-#define DGBGK_EMESH (-2)     /* inconsistent mesh (side or wall not found) */
+#define DGBGK_EMESH (-2)     /* inconsistent mesh (node out of range, side or wall not found, zero area or length) */
 #define DGBGK_ECUDA (-3)     /* CUDA runtime error or no usable sm_100 GPU */
 #define DGBGK_ENONFINITE (-4) /* non-finite residual: the state diverged */
 #define DGBGK_EUNSUP (-5)    /* configuration not supported by this build */

@@ -1,6 +1,7 @@
 // sm_100a kernels of the DG-BGK pseudo-time step.
 //
-// One step (src/advnce.f90:220-400) is four launches on one stream:
+// One step (src/advnce.f90:220-400) is four launches on one stream (five
+// with ALPHA < 1: k_wspec after the sweep):
 //   k_moments : MACROS passes 1+2 (src/macros.f90:80-154) fused with COMPMU
 //               (src/compmu.f90:242-290) and the GTEQNF parameters
 //               (src/gteqnf.f90:315-326).  Persistent warps take R whole
@@ -8,7 +9,7 @@
 //               per-warp ring of stages filled by 1-D bulk copies, so f is
 //               read from HBM once for both passes; every access is a
 //               16-byte vector.
-//   k_wall    : FLUCON2 (src/flucon2.f90:134-233), one warp per wall side.
+//   k_wall    : FLUCON2 (src/flucon2.f90:134-233), one CTA per wall side.
 //   k_sweep   : the whole velocity-loop body (GTEQNF, GETFLA, GETELC,
 //               EDGFLXOPT/GETBOU, GETINC/CMMINC, ADTHEM, INFLOW;
 //               src/advnce.f90:286-377) on tiles of (element block x one

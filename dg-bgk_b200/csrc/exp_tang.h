@@ -63,7 +63,8 @@ DGBGK_HD double exp_tang(double x, const double* __restrict__ tab) {
   const double t = tab[k & (EXP_TAB - 1)];
   const double y = fma(t, p, t);
   const int64_t m = (int64_t)(k >> 6);  // floor(k / 64)
-  const double v = dbl_from_bits(dbl_bits(y) + (m << 52));
+  // 2^m: m added to the exponent field (two's complement, shifted unsigned)
+  const double v = dbl_from_bits((int64_t)((uint64_t)dbl_bits(y) + ((uint64_t)m << 52)));
   return x > -707.0 ? v : (x != x ? x : 0.0);
 }
 

@@ -28,7 +28,8 @@ int main() {
   };
   for (int i = 0; i < 2000000; ++i) { check(wide(g)); check(near(g)); check(small(g)); }
   // every table boundary and half-way point over [-706, 0]
-  for (int k = -65200; k <= 0; ++k) { check(k * (0.6931471805599453 / 64)); check((k + 0.5) * (0.6931471805599453 / 64)); }
+  const double step = 0.6931471805599453 / 64;
+  for (int k = -65200; k <= 0; ++k) { check(k * step); check((k + 0.5) * step); }
   check(0.0); check(-0.0); check(-706.99);
   const double flushed = dgbgk::exp_tang(-707.5, tab), nan_in = dgbgk::exp_tang(NAN, tab);
   const double neg_inf = dgbgk::exp_tang(-INFINITY, tab);

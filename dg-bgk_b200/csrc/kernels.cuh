@@ -649,6 +649,67 @@ __device__ __forceinline__ void sweep_p1(const ElemRec<T>& r, const double* etab
   for (int i = 0; i < 3; ++i) vst<T>(row[i], f[i]);
 }
 
+// FP32 phase 1 on packed pairs of velocities (fma.rn.f32x2, mul/add.f32x2:
+// one instruction per two velocities of an element, the element's
+// coefficients broadcast to both halves), the same operations per value as
+// the generic sweep_p1.  Built only with DGBGK_SWEEP_PACKED32=1: it compiles
+// to the same 128 registers without spills in the single-case sweep, and is
+// kept out of the default build until measured on the GPU.
+#ifndef DGBGK_SWEEP_PACKED32
+#define DGBGK_SWEEP_PACKED32 0
+#endif
+#if DGBGK_SWEEP_PACKED32
+__device__ __forceinline__ float2 bc2(float x) { return make_float2(x, x); }
+template <>
+__device__ __forceinline__ void sweep_p1<float>(const ElemRec<float>& r, const double* etab, unsigned char* tl, int r0,
+                                                int c, const float4& cxv, const float4& cyv, float dth, float dth3,
+                                                float4 (&q)[3], float4& u) {
+  unsigned char* row[3];
+  float4 f4[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    row[i] = tl + tile_off(r0 + i, c);
+    f4[i] = vld<float>(row[i]);
+  }
+  const float2 m1 = bc2(-1.0f);
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const float2 cx = h ? make_float2(cxv.z, cxv.w) : make_float2(cxv.x, cxv.y);
+    const float2 cy = h ? make_float2(cyv.z, cyv.w) : make_float2(cyv.x, cyv.y);
+    float2 f[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) f[i] = h ? make_float2(f4[i].z, f4[i].w) : make_float2(f4[i].x, f4[i].y);
+    float2 sx = __fmul2_rn(bc2(r.gx[0]), f[0]);
+    sx = __ffma2_rn(bc2(r.gx[1]), f[1], sx);
+    sx = __ffma2_rn(bc2(r.gx[2]), f[2], sx);
+    float2 sy = __fmul2_rn(bc2(r.gy[0]), f[0]);
+    sy = __ffma2_rn(bc2(r.gy[1]), f[1], sy);
+    sy = __ffma2_rn(bc2(r.gy[2]), f[2], sy);
+    float2 coll = bc2(0.0f);
+    float2 qq[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const float2 dx = __ffma2_rn(cx, m1, bc2(r.ux[i]));
+      const float2 dy = __ffma2_rn(cy, m1, bc2(r.uy[i]));
+      const float2 arg = __fmul2_rn(bc2(r.ex[i]), __ffma2_rn(dx, dx, __fmul2_rn(dy, dy)));
+      qq[i] = __fmul2_rn(bc2(r.A[i]), make_float2(nfo_exp<float>(arg.x, etab), nfo_exp<float>(arg.y, etab)));
+      coll = __ffma2_rn(bc2(r.mu[i]), __ffma2_rn(f[i], m1, qq[i]), coll);
+    }
+    float2 um = __fmul2_rn(bc2(dth), __ffma2_rn(sy, cy, __fmul2_rn(sx, cx)));
+    um = __ffma2_rn(bc2(-dth3), coll, um);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const float2 g = __ffma2_rn(um, m1, f[i]);
+      if (h) { q[i].z = qq[i].x; q[i].w = qq[i].y; f4[i].z = g.x; f4[i].w = g.y; }
+      else { q[i].x = qq[i].x; q[i].y = qq[i].y; f4[i].x = g.x; f4[i].y = g.y; }
+    }
+    if (h) { u.z = um.x; u.w = um.y; } else { u.x = um.x; u.y = um.y; }
+  }
+#pragma unroll
+  for (int i = 0; i < 3; ++i) vst<float>(row[i], f4[i]);
+}
+#endif  // DGBGK_SWEEP_PACKED32
+
 // Persistent sweep kernel: EB block elements, TPE*EB threads.  Work units are
 // (block b, group of `tpu` velocity tiles) with b fastest, handed out in
 // order (the first by blockIdx, the rest from a device counter), so the CTAs

@@ -652,9 +652,9 @@ __device__ __forceinline__ void sweep_p1(const ElemRec<T>& r, const double* etab
 // FP32 phase 1 on packed pairs of velocities (fma.rn.f32x2, mul/add.f32x2:
 // one instruction per two velocities of an element, the element's
 // coefficients broadcast to both halves), the same operations per value as
-// the generic sweep_p1.  Built only with DGBGK_SWEEP_PACKED32=1: it compiles
-// to the same 128 registers without spills in the single-case sweep, and is
-// kept out of the default build until measured on the GPU.
+// the generic sweep_p1.  Built only with DGBGK_SWEEP_PACKED32 >= 1: it
+// compiles to the same 128 registers without spills in the single-case
+// sweep, and is kept out of the default build until measured on the GPU.
 #ifndef DGBGK_SWEEP_PACKED32
 #define DGBGK_SWEEP_PACKED32 0
 #endif
@@ -708,6 +708,52 @@ __device__ __forceinline__ void sweep_p1<float>(const ElemRec<float>& r, const d
 #pragma unroll
   for (int i = 0; i < 3; ++i) vst<float>(row[i], f4[i]);
 }
+
+#if DGBGK_SWEEP_PACKED32 >= 2
+// Volume and edge terms of one 16-byte chunk (four velocities) on packed
+// pairs: RHS_i = AREA/3 (N_i,x cx + N_i,y cy) sum(g) and the upwind edge
+// fluxes, the same operations per value as the generic loops of k_sweep;
+// the upwind choice stays per velocity.  Level 2 of DGBGK_SWEEP_PACKED32
+// (with it the single-case FP32 sweep spills 36 bytes at 128 registers).
+__device__ __forceinline__ void sweep_rhs_packed(const ElemRec<float>& r, float area3, const float4& cxv,
+                                                 const float4& cyv, const float4 (&g)[3], const unsigned char* tl,
+                                                 const unsigned (&srcp)[3], const unsigned (&srcq)[3], unsigned cx16,
+                                                 const float (&anx)[3], const float (&any)[3], float (&rhs)[3][4]) {
+  const float2 m1 = bc2(-1.0f), two = bc2(2.0f);
+  auto pr = [](const float4& v, int h) { return h ? make_float2(v.z, v.w) : make_float2(v.x, v.y); };
+  float2 rr[2][3];
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const float2 cx = pr(cxv, h), cy = pr(cyv, h);
+    const float2 s3 = __fmul2_rn(__fadd2_rn(__fadd2_rn(pr(g[0], h), pr(g[1], h)), pr(g[2], h)), bc2(area3));
+    rr[h][0] = __fmul2_rn(__ffma2_rn(bc2(r.gx[0]), cx, __fmul2_rn(bc2(r.gy[0]), cy)), s3);
+    rr[h][1] = __fmul2_rn(__ffma2_rn(bc2(r.gx[1]), cx, __fmul2_rn(bc2(r.gy[1]), cy)), s3);
+    rr[h][2] = __fmul2_rn(__fadd2_rn(rr[h][0], rr[h][1]), m1);
+  }
+#pragma unroll
+  for (int k2 = 0; k2 < 3; ++k2) {
+    const int p = k2, qn = (k2 + 1) % 3;
+    const float4 gp4 = vld<float>(tl + (srcp[k2] ^ cx16)), gq4 = vld<float>(tl + (srcq[k2] ^ cx16));
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const float2 as = __ffma2_rn(bc2(anx[k2]), pr(cxv, h), __fmul2_rn(bc2(any[k2]), pr(cyv, h)));
+      const float2 gp = pr(gp4, h), gq = pr(gq4, h), op = pr(g[p], h), oq = pr(g[qn], h);
+      const float2 up = make_float2(as.x > 0.0f ? op.x : gp.x, as.y > 0.0f ? op.y : gp.y);
+      const float2 uq = make_float2(as.x > 0.0f ? oq.x : gq.x, as.y > 0.0f ? oq.y : gq.y);
+      const float2 nas = __fmul2_rn(as, m1);
+      rr[h][p] = __ffma2_rn(nas, __ffma2_rn(two, up, uq), rr[h][p]);
+      rr[h][qn] = __ffma2_rn(nas, __ffma2_rn(two, uq, up), rr[h][qn]);
+    }
+  }
+#pragma unroll
+  for (int h = 0; h < 2; ++h)
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      rhs[i][2 * h] = rr[h][i].x;
+      rhs[i][2 * h + 1] = rr[h][i].y;
+    }
+}
+#endif  // DGBGK_SWEEP_PACKED32 >= 2
 #endif  // DGBGK_SWEEP_PACKED32
 
 // Persistent sweep kernel: EB block elements, TPE*EB threads.  Work units are
@@ -954,27 +1000,34 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : (E
             // = cx * mean(g), FYME = cy * mean(g); the P1 gradients sum to
             // zero, so RHS_3 = -(RHS_1 + RHS_2)
             T rhs[3][W];
-#pragma unroll
-            for (int w = 0; w < W; ++w) {
-              const T cx = VO::get(cxv, w), cy = VO::get(cyv, w);
-              const T s3 = (VO::get(g[0], w) + VO::get(g[1], w) + VO::get(g[2], w)) * area3;
-              rhs[0][w] = (r.gx[0] * cx + r.gy[0] * cy) * s3;
-              rhs[1][w] = (r.gx[1] * cx + r.gy[1] * cy) * s3;
-              rhs[2][w] = -(rhs[0][w] + rhs[1][w]);
-            }
-            // edge fluxes: RHS_p -= AL*SC*(2 u_p + u_q), RHS_q -= AL*SC*(u_p + 2 u_q)
-#pragma unroll
-            for (int k2 = 0; k2 < 3; ++k2) {
-              const int p = k2, qn = (k2 + 1) % 3;
-              const VecT gp = vld<T>(tl + (srcp[k2] ^ cx16)), gq = vld<T>(tl + (srcq[k2] ^ cx16));
+#if DGBGK_SWEEP_PACKED32 >= 2
+            if constexpr (sizeof(T) == 4) {
+              sweep_rhs_packed(r, area3, cxv, cyv, g, tl, srcp, srcq, cx16, anx, any, rhs);
+            } else
+#endif
+            {
 #pragma unroll
               for (int w = 0; w < W; ++w) {
-                const T as = anx[k2] * VO::get(cxv, w) + any[k2] * VO::get(cyv, w);
-                const bool mine = as > (T)0;
-                const T up = mine ? VO::get(g[p], w) : VO::get(gp, w);
-                const T uq = mine ? VO::get(g[qn], w) : VO::get(gq, w);
-                rhs[p][w] -= as * ((T)2 * up + uq);
-                rhs[qn][w] -= as * (up + (T)2 * uq);
+                const T cx = VO::get(cxv, w), cy = VO::get(cyv, w);
+                const T s3 = (VO::get(g[0], w) + VO::get(g[1], w) + VO::get(g[2], w)) * area3;
+                rhs[0][w] = (r.gx[0] * cx + r.gy[0] * cy) * s3;
+                rhs[1][w] = (r.gx[1] * cx + r.gy[1] * cy) * s3;
+                rhs[2][w] = -(rhs[0][w] + rhs[1][w]);
+              }
+              // edge fluxes: RHS_p -= AL*SC*(2 u_p + u_q), RHS_q -= AL*SC*(u_p + 2 u_q)
+#pragma unroll
+              for (int k2 = 0; k2 < 3; ++k2) {
+                const int p = k2, qn = (k2 + 1) % 3;
+                const VecT gp = vld<T>(tl + (srcp[k2] ^ cx16)), gq = vld<T>(tl + (srcq[k2] ^ cx16));
+#pragma unroll
+                for (int w = 0; w < W; ++w) {
+                  const T as = anx[k2] * VO::get(cxv, w) + any[k2] * VO::get(cyv, w);
+                  const bool mine = as > (T)0;
+                  const T up = mine ? VO::get(g[p], w) : VO::get(gp, w);
+                  const T uq = mine ? VO::get(g[qn], w) : VO::get(gq, w);
+                  rhs[p][w] -= as * ((T)2 * up + uq);
+                  rhs[qn][w] -= as * (up + (T)2 * uq);
+                }
               }
             }
             // ALPHA < 1: bit 3*w + i marks node i at velocity vb + w as

@@ -107,6 +107,16 @@ SIGNATURES = {
 _lib = None
 
 
+def use_library(path):
+    """Loads the library from `path` (another build of the same ABI, e.g. a
+    compile-time variant) instead of lib/libdgbgk.so; call before the first
+    use."""
+    global LIB_PATH
+    if _lib is not None:
+        raise RuntimeError("the library is already loaded from " + LIB_PATH)
+    LIB_PATH = os.path.abspath(path)
+
+
 def lib():
     """Loads libdgbgk.so once; raises if it has not been built."""
     global _lib

@@ -47,3 +47,18 @@ def test_create_without_gpu_fails_loudly():
         Solver.from_case(cavity_case(4, 4, 8))
     assert ei.value.code == DGBGK_ECUDA
     assert "no CPU fallback" in str(ei.value) or "CUDA" in str(ei.value)
+
+
+def test_another_build_of_the_abi_can_be_chosen_before_loading():
+    # `python -m dgbgk.profile --lib ...` times a compile-time variant
+    # (`make variant`); the choice is refused once a library is loaded
+    import subprocess
+    import sys
+    code = ("import dgbgk._lib as L, os; L.use_library('variant.so'); print(L.LIB_PATH); "
+            "L.use_library(os.path.join(os.path.dirname(L.__file__), '..', 'lib', 'libdgbgk.so')); L.lib()\n"
+            "try:\n    L.use_library('other.so')\nexcept RuntimeError as e:\n    print('refused')")
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, cwd=ROOT,
+                       env=dict(os.environ, PYTHONPATH=os.path.join(ROOT, "dg-bgk_b200")))
+    assert r.returncode == 0, r.stderr
+    out = r.stdout.split()
+    assert out[0] == os.path.join(ROOT, "variant.so") and out[1] == "refused"

@@ -97,6 +97,12 @@ struct ImplBase {
   int nsm = 148;
   double ref_host = 0.0;
   float last_ms = 0.f;
+  // bumped when the case's device table entry changes (buffers moved,
+  // re-blocked): a batch holding the case rebuilds its table
+  unsigned gen = 0;
+  // bumped when the state is written from outside the time loop: a batch
+  // lets a case it stopped after a divergence run again
+  unsigned epoch = 0;
 };
 
 // A set of cases launched together (one handle, or a batch): the case table
@@ -587,6 +593,7 @@ template <class T> struct Impl : ImplBase {
 
   // the one-case launch set
   int refresh() {
+    ++gen;
     fill_case();
     TRY(build_launch_set(single, std::vector<CaseDev<T>>{hc}, pl.EB, pl.immat, pl.max_halo, nsm, st));
     drop_graphs();
@@ -792,6 +799,7 @@ template <class T> struct Impl : ImplBase {
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(st));
     cur = 0;
+    ++epoch;
     return 0;
   }
   int get_state(void* dst, bool f32) override {
@@ -824,6 +832,7 @@ template <class T> struct Impl : ImplBase {
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(st));
     cur = 0;
+    ++epoch;
     return 0;
   }
   int snapshot(int slot) override {
@@ -915,6 +924,7 @@ template <class T> struct Impl : ImplBase {
     k_combine<T><<<grid, 256, 0, st>>>(snaps, N, m, d_gamma, N, f[cur]);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(st));
+    ++epoch;
     return 0;
   }
   int upload_perm() {
@@ -969,6 +979,7 @@ template <class T> struct Impl : ImplBase {
     if (dsc) cudaFree(dsc);
     CK(e);
     cur = 0;
+    ++epoch;
     return 0;
   }
 
@@ -993,6 +1004,7 @@ template <class T> struct Impl : ImplBase {
     cudaFree(dp);
     CK(e);
     cur = 0;
+    ++epoch;
     return 0;
   }
 
@@ -1301,6 +1313,7 @@ struct BatchBase {
   virtual int tuning(int n, double* ms) const = 0;
   float last_ms = 0.f;
   std::vector<int> last_rc;  // per case: the status of the last advance
+  std::vector<int> active;   // per case: 0 = left out of the advances (dgbgk_batch_set_active)
 };
 
 template <class T> struct BatchImpl : BatchBase {
@@ -1317,6 +1330,12 @@ template <class T> struct BatchImpl : BatchBase {
   // ms per step: (eb 64, 128) x (upc 2, 4, 8, 16), then moment rows 1, 2, 4;
   // 0 = not tried
   std::vector<double> tune_ms;
+  // per case: the handle's table generation the launch set was built from
+  std::vector<unsigned> gens;
+  // per case: a non-zero status that stops the case (divergence, expired
+  // wait) and the state epoch it belongs to; a new state clears it
+  std::vector<int> stop_rc;
+  std::vector<unsigned> stop_epoch;
 
   ~BatchImpl() override {
     cudaSetDevice(device);
@@ -1351,7 +1370,18 @@ template <class T> struct BatchImpl : BatchBase {
     TRY(dalloc(&d_done, 1));
     CK(cudaMallocHost((void**)&h_done, 2 * sizeof(int)));
     tune_ms.assign(11, 0.0);
+    active.assign(cs.size(), 1);
+    stop_rc.assign(cs.size(), 0);
+    stop_epoch.assign(cs.size(), 0);
+    last_rc.assign(cs.size(), 0);
     return 0;
+  }
+
+  // the case runs in the next advance: active and not stopped (a stop
+  // lapses once the case's state was written anew)
+  bool runs(size_t i) {
+    if (stop_rc[i] != 0 && stop_epoch[i] != cs[i]->epoch) stop_rc[i] = 0;
+    return active[i] && stop_rc[i] == 0;
   }
 
   // Re-blocks every case to EB = e and gives each case its tiles per unit
@@ -1378,6 +1408,8 @@ template <class T> struct BatchImpl : BatchBase {
       table.push_back(c->hc);
     }
     TRY(build_launch_set(L, table, e, immat, max_halo, nsm, st, rows));
+    gens.clear();
+    for (auto* c : cs) gens.push_back(c->gen);
     eb = e;
     upc = u;
     if (gexec) {
@@ -1387,9 +1419,13 @@ template <class T> struct BatchImpl : BatchBase {
     return 0;
   }
 
+  // every case's control block for an advance; a case that does not run
+  // is uploaded finished (the kernels skip it; its step count stays 0)
   int upload_ctrls(int max_steps, double tol) {
-    for (auto* c : cs) {
+    for (size_t i = 0; i < cs.size(); ++i) {
+      Impl<T>* c = cs[i];
       c->fill_ctrl(c->hctrl[0], max_steps, tol);
+      if (!runs(i)) c->hctrl[0].done = 1;
       CK(cudaMemcpyAsync(c->ctrl, &c->hctrl[0], sizeof(Ctrl), cudaMemcpyHostToDevice, st));
     }
     return 0;
@@ -1398,7 +1434,7 @@ template <class T> struct BatchImpl : BatchBase {
   // Autotuner: times `steps` steps (after one untimed) of every candidate
   // tile shape on the cases' current states, restoring the states after
   // each, and keeps the fastest.
-  int autotune(int fixed_eb, int fixed_upc, int steps) {
+  int autotune(int fixed_eb, int fixed_upc, int fixed_rows, int steps) {
     std::vector<T*> backup(cs.size(), nullptr);
     int rc = 0;
     for (size_t i = 0; i < cs.size() && rc == 0; ++i) {
@@ -1457,6 +1493,7 @@ template <class T> struct BatchImpl : BatchBase {
     int brows = 0;
     best = 1e300;
     for (int ir = 0; ir < 3 && rc == 0; ++ir) {
+      if (fixed_rows > 0 && rws[ir] != fixed_rows) continue;
       rows = rws[ir];
       rc = configure(beb, bupc);
       if (rc == DGBGK_EUNSUP) {
@@ -1499,13 +1536,14 @@ template <class T> struct BatchImpl : BatchBase {
       return DGBGK_EINVAL;
     }
     CK(cudaSetDevice(device));
-    bool rebuilt = false;
     for (auto* c : cs)
-      if (c->hist_cap < max_steps) {
-        TRY(c->ensure_hist(max_steps));
-        rebuilt = true;
-      }
-    if (rebuilt) TRY(configure(eb, upc));
+      if (c->hist_cap < max_steps) TRY(c->ensure_hist(max_steps));
+    // a case's table entry changed since the launch set was built (its
+    // history grew above, or it was re-blocked or grown on its own or by
+    // another batch): rebuild the table before any launch reads it
+    bool stale = gens.size() != cs.size();
+    for (size_t i = 0; i < cs.size() && !stale; ++i) stale = gens[i] != cs[i]->gen;
+    if (stale) TRY(configure(eb, upc));
     for (auto* c : cs) CK(cudaStreamSynchronize(c->st));
     TRY(build_graph());
     TRY(upload_ctrls(max_steps, tol));
@@ -1535,16 +1573,25 @@ template <class T> struct BatchImpl : BatchBase {
     last_rc.assign(cs.size(), 0);
     for (size_t i = 0; i < cs.size(); ++i) {
       Impl<T>* c = cs[i];
+      if (steps) steps[i] = 0;
+      if (l2) l2[i] = 0.0;
+      if (!active[i]) continue;
+      if (stop_rc[i] != 0) {  // stopped before this advance: keeps its status
+        last_rc[i] = stop_rc[i];
+        if (rc == 0) rc = stop_rc[i];
+        continue;
+      }
       CK(cudaMemcpy(&c->hctrl[1], c->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost));
       int ns = 0;
       const int r = c->collect(c->hctrl[1], &ns, nullptr, nullptr, nullptr);
       last_rc[i] = r;
-      if (r != 0 && rc == 0) rc = r;
-      if (steps) steps[i] = ns;
-      if (l2) {
-        l2[i] = 0.0;
-        if (ns > 0) CK(cudaMemcpy(&l2[i], c->hist_l2 + ns - 1, sizeof(double), cudaMemcpyDeviceToHost));
+      if (r != 0) {
+        stop_rc[i] = r;
+        stop_epoch[i] = c->epoch;
+        if (rc == 0) rc = r;
       }
+      if (steps) steps[i] = ns;
+      if (l2 && ns > 0) CK(cudaMemcpy(&l2[i], c->hist_l2 + ns - 1, sizeof(double), cudaMemcpyDeviceToHost));
     }
     return rc;
   }
@@ -1577,6 +1624,7 @@ void dgbgk_batch_default_params(dgbgk_batch_params* p) {
   p->tile_elems = 0;
   p->units_per_cta = 0;
   p->tune_steps = 4;
+  p->moment_rows = 0;
 }
 
 int dgbgk_batch_create(dgbgk_handle* const* cases, int ncases, const dgbgk_batch_params* prm,
@@ -1609,14 +1657,14 @@ int dgbgk_batch_create(dgbgk_handle* const* cases, int ncases, const dgbgk_batch
     std::vector<Impl<double>*> v;
     for (int i = 0; i < ncases; ++i) v.push_back(static_cast<Impl<double>*>(cases[i]->impl.get()));
     rc = bi->init(v);
-    if (rc == 0) rc = bi->autotune(p.tile_elems, p.units_per_cta, std::max(1, p.tune_steps));
+    if (rc == 0) rc = bi->autotune(p.tile_elems, p.units_per_cta, p.moment_rows, std::max(1, p.tune_steps));
   } else {
     auto* bi = new BatchImpl<float>();
     b.reset(bi);
     std::vector<Impl<float>*> v;
     for (int i = 0; i < ncases; ++i) v.push_back(static_cast<Impl<float>*>(cases[i]->impl.get()));
     rc = bi->init(v);
-    if (rc == 0) rc = bi->autotune(p.tile_elems, p.units_per_cta, std::max(1, p.tune_steps));
+    if (rc == 0) rc = bi->autotune(p.tile_elems, p.units_per_cta, p.moment_rows, std::max(1, p.tune_steps));
   }
   if (rc != 0) return rc;
   *out = new dgbgk_batch{std::move(b)};
@@ -1626,6 +1674,12 @@ int dgbgk_batch_create(dgbgk_handle* const* cases, int ncases, const dgbgk_batch
 int dgbgk_batch_advance(dgbgk_batch* b, int max_steps, double tol, int* steps_done, double* res_l2_last) {
   if (!b || !b->impl) return set_error("NULL batch"), DGBGK_EINVAL;
   return b->impl->advance(max_steps, tol, steps_done, res_l2_last);
+}
+
+int dgbgk_batch_set_active(dgbgk_batch* b, const int* active) {
+  if (!b || !b->impl || !active) return set_error("NULL batch"), DGBGK_EINVAL;
+  for (size_t i = 0; i < b->impl->active.size(); ++i) b->impl->active[i] = active[i] != 0;
+  return DGBGK_OK;
 }
 
 int dgbgk_batch_status(const dgbgk_batch* b, int* status) {

@@ -528,6 +528,14 @@ __device__ __forceinline__ unsigned tile_off(int r, int c) {
   return (unsigned)(r * 64 + 16 * (c ^ ((r >> 1) & 3)));
 }
 
+// A tensor map read from global memory (the batch's case table, written by
+// a host copy) must be acquired by the tensormap proxy before a thread uses
+// it; one fence per map and thread.  Maps passed as __grid_constant__
+// parameters need none.
+__device__ __forceinline__ void tensormap_acquire(const CUtensorMap* p) {
+  asm volatile("fence.proxy.tensormap::generic.acquire.sys [%0], 128;" ::"l"(p) : "memory");
+}
+
 // 2-D tiled TMA load (no multicast) of one box into shared memory.
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
   asm volatile(
@@ -796,7 +804,12 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : (E
   constexpr unsigned BOX_BYTES = G::BOX_ROWS * 64;
   static_assert(EB % 16 == 0, "whole warps");
   extern __shared__ __align__(128) unsigned char sm_raw[];
-  __shared__ int s_unit;
+  // the next unit, handed from thread 0 to the CTA: two slots used in turn,
+  // so thread 0 never overwrites the slot another warp may still be reading
+  // (a unit of a finished case has no barrier of its own: with one slot,
+  // thread 0 could loop round and replace the value before a slow warp read
+  // it, and the warps would then disagree on the unit and on the barriers)
+  __shared__ int s_unit[2];
   __shared__ double red_m[NW], red_s[NW];
   __shared__ uint64_t bars[2];  // TMA completion of tile buffer 0 / 1
   // FP64: the 2^(j/64) table of the NFO exp (one entry for FP32, unused)
@@ -833,13 +846,17 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : (E
     bulk_commit();
   };
 
-  int unit = blockIdx.x, c = 0;
+  int unit = blockIdx.x, c = 0, iter = 0;
   // the unit after this one, drawn ahead so the atomic's latency is hidden
   int next = (tid == 0 && unit < total_units) ? (int)gridDim.x + atomicAdd(&a.ctl->sweep_next, 1) : 0;
   while (unit < total_units) {
     c = ONE ? 0 : find_case(a.unit_off, a.ncases, unit);
     const CaseDev<T>& C = ONE ? one : a.cases[c];
     const bool active = !C.ctrl->done;  // the same for every thread
+    if (!ONE && active && tid == 0) {
+      tensormap_acquire(&C.tm[0]);
+      tensormap_acquire(&C.tm[1]);
+    }
     const CUtensorMap* last_map = nullptr;
     int last_vt = 0, last_bi = 0, last_y0 = 0;
     if (active) {
@@ -1181,7 +1198,7 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : (E
     // (the sum of squares can differ in its last bits between runs: the
     // order of the atomics varies); the records, tables and halo list may
     // be replaced
-    if (tid == 0) s_unit = next;
+    if (tid == 0) s_unit[iter & 1] = next;
     __syncthreads();
     if (tid == 0 && last_map) {
       store(last_map, last_vt, last_bi, last_y0);
@@ -1193,7 +1210,8 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : (E
       atomicAdd(&C.ctrl->acc_sq, ss);
       atomicMax(reinterpret_cast<unsigned long long*>(&C.ctrl->acc_max), (unsigned long long)__double_as_longlong(mm));
     }
-    unit = s_unit;
+    unit = s_unit[iter & 1];
+    ++iter;
     if (tid == 0 && unit < total_units) next = (int)gridDim.x + atomicAdd(&a.ctl->sweep_next, 1);
   }
   if (tid == 0) bulk_wait0();  // the last box stores are complete before the CTA exits

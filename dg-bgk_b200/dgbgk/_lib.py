@@ -52,7 +52,7 @@ class Params(ctypes.Structure):
 
 
 class BatchParams(ctypes.Structure):
-    _fields_ = [("tile_elems", c_int), ("units_per_cta", c_int), ("tune_steps", c_int)]
+    _fields_ = [("tile_elems", c_int), ("units_per_cta", c_int), ("tune_steps", c_int), ("moment_rows", c_int)]
 
 
 # name -> (restype, argtypes); mirrors include/dgbgk.h
@@ -88,6 +88,7 @@ SIGNATURES = {
     "dgbgk_batch_default_params": (None, [POINTER(BatchParams)]),
     "dgbgk_batch_create": (c_int, [POINTER(c_void_p), c_int, POINTER(BatchParams), POINTER(c_void_p)]),
     "dgbgk_batch_advance": (c_int, [c_void_p, c_int, c_double, _PI, _PD]),
+    "dgbgk_batch_set_active": (c_int, [c_void_p, _PI]),
     "dgbgk_batch_status": (c_int, [c_void_p, _PI]),
     "dgbgk_batch_info": (c_int, [c_void_p, _PI]),
     "dgbgk_batch_tuning": (c_int, [c_void_p, c_int, _PD]),

@@ -179,15 +179,20 @@ class Solver:
         check(lib().dgbgk_init_maxwellian(self.h, *(ptr(x) for x in a)))
 
     # -- time loop ----------------------------------------------------
-    def advance(self, nsteps, tol=0.0):
+    def advance(self, nsteps, tol=0.0, raise_on_error=True):
+        """Runs up to nsteps steps (to tol relative to the residual
+        reference when tol > 0).  With raise_on_error=False a failed advance
+        returns its status in "rc" (the steps run before it, and their
+        residuals, are kept)."""
         linf = np.zeros(max(nsteps, 1))
         l2 = np.zeros(max(nsteps, 1))
         dte = np.zeros(max(nsteps, 1))
         done = c_int(0)
         rc = lib().dgbgk_advance(self.h, nsteps, tol, ctypes.byref(done), ptr(linf), ptr(l2), ptr(dte))
         n = done.value
-        res = {"steps": n, "res_linf": linf[:n], "res_l2": l2[:n], "dte": dte[:n]}
-        check(rc)
+        res = {"steps": n, "res_linf": linf[:n], "res_l2": l2[:n], "dte": dte[:n], "rc": rc}
+        if raise_on_error:
+            check(rc)
         return res
 
     def last_ms(self):
@@ -257,7 +262,7 @@ class Batch:
 
     TUNE_KEYS = [(eb, upc) for eb in (64, 128) for upc in (2, 4, 8, 16)] + [("rows", r) for r in (1, 2, 4)]
 
-    def __init__(self, solvers, tile_elems=0, units_per_cta=0, tune_steps=4):
+    def __init__(self, solvers, tile_elems=0, units_per_cta=0, tune_steps=4, moment_rows=0):
         from ._lib import BatchParams
         self.solvers = list(solvers)
         p = BatchParams()
@@ -265,10 +270,13 @@ class Batch:
         p.tile_elems = tile_elems
         p.units_per_cta = units_per_cta
         p.tune_steps = tune_steps
+        p.moment_rows = moment_rows
         hs = (c_void_p * len(self.solvers))(*[s.h for s in self.solvers])
         b = c_void_p()
         check(lib().dgbgk_batch_create(hs, len(self.solvers), ctypes.byref(p), ctypes.byref(b)))
         self.h = b
+        # the autotuner's choice, kept for the record
+        self.shape = self.info()
 
     def advance(self, max_steps, tol=0.0, raise_on_error=True):
         """Steps every case to tol (relative to its reference) or max_steps.
@@ -284,6 +292,18 @@ class Batch:
         if rc != 0 and (raise_on_error or not diverged_only):
             check(rc)
         return {"steps": steps, "res_l2_last": l2, "status": status}
+
+    def set_active(self, active):
+        """Leaves the cases with active[i] false out of the following
+        advances (0 steps, state untouched)."""
+        a = np.ascontiguousarray(np.asarray(active, dtype=bool).astype(np.int32))
+        assert a.size == len(self.solvers)
+        check(lib().dgbgk_batch_set_active(self.h, ptr(a, c_int)))
+
+    def shape_record(self):
+        """The tile shape in use: elements per CTA, units per CTA and moment
+        rows per warp step."""
+        return {k: self.shape[k] for k in ("tile_elems", "units_per_cta", "moment_rows")}
 
     def info(self):
         o = np.zeros(7, dtype=np.int32)

@@ -133,27 +133,32 @@ def march_batch(b, solvers, tol, max_steps, chunk=1000, stall=0.8, stall_below=1
     reference), has stalled (below stall_below, its residual fell by less
     than the factor `stall` over the last chunk: an FP32 march at its
     rounding plateau; the transient's residual may rise for a while above
-    that), has diverged, or max_steps have run.  Returns steps per case, the
-    last relative residuals, the statuses and the device seconds."""
+    that), has diverged, or max_steps have run.  A finished case is left
+    out of the following chunks (dgbgk_batch_set_active).  Returns steps per
+    case, the last relative residuals, the statuses and the device
+    seconds."""
     n = len(solvers)
     steps = np.zeros(n, dtype=np.int64)
     status = np.zeros(n, dtype=np.int32)
     prev = np.full(n, np.inf)
     rel = np.full(n, np.inf)
+    done = np.zeros(n, dtype=bool)
     dev = 0.0
     while steps.max() < max_steps:
         r = b.advance(min(chunk, max_steps - int(steps.max())), tol=tol, raise_on_error=False)
         dev += b.last_ms() * 1e-3
-        live = status == 0
+        live = (status == 0) & ~done
         steps[live] += r["steps"][live]
         status[live] = r["status"][live]
         refs = np.array([s.residual_reference() for s in solvers])
         now = r["res_l2_last"] / np.maximum(refs, 1e-300)
         rel = np.where(live & (r["steps"] > 0), now, rel)
-        done = (rel <= tol * (1 + 1e-9)) | (status != 0) | ((rel > stall * prev) & (rel < stall_below))
+        done |= (rel <= tol * (1 + 1e-9)) | (status != 0) | ((rel > stall * prev) & (rel < stall_below))
         prev = np.where(live, rel, prev)
         if done.all():
             break
+        b.set_active(~done)
+    b.set_active(np.ones(n, dtype=bool))
     return steps, rel, status, dev
 
 
@@ -177,6 +182,7 @@ def march_batch_rre(b, solvers, tol, max_steps, start=1e-2, every=100, m=8, stal
     refs = np.array([s.residual_reference() for s in solvers])
 
     def adv(k):
+        b.set_active(~done)
         r = b.advance(k, tol=tol, raise_on_error=False)
         dev[0] += b.last_ms() * 1e-3
         live = (status == 0) & ~done
@@ -219,6 +225,7 @@ def march_batch_rre(b, solvers, tol, max_steps, start=1e-2, every=100, m=8, stal
                 use[i] = False
     for s in solvers:
         s.snapshot(-1)
+    b.set_active(np.ones(n, dtype=bool))
     return steps, rel.copy(), status, dev[0]
 
 
@@ -250,7 +257,7 @@ def generate(cases, precision=32, tol=1e-5, accept=1e-4, group=64, max_steps=600
         if log:
             log(f"generate rank {rank}/{world} {g0}..{g0 + len(part)}: steps {int(steps.min())}..{int(steps.max())} "
                 f"diverged {int((status != 0).sum())} kept {int(((status == 0) & (rel <= accept)).sum())} "
-                f"device {dev:.1f} s wall {time.perf_counter() - t:.1f} s")
+                f"device {dev:.1f} s wall {time.perf_counter() - t:.1f} s shape {b.shape_record()}")
         for k, (c, s) in enumerate(zip(part, ss)):
             if status[k] == 0 and rel[k] <= accept:
                 q = nodal_fields(s, c)

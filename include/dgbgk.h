@@ -229,6 +229,7 @@ typedef struct {
   int tile_elems;     /* sweep elements per CTA, 64 or 128 (0: autotuned)    */
   int units_per_cta;  /* sweep work units per resident CTA, 2/4/8/16 (0: autotuned) */
   int tune_steps;     /* steps timed per autotuner candidate                */
+  int moment_rows;    /* moment rows per warp step, 1/2/4 (0: autotuned)     */
 } dgbgk_batch_params;
 
 void dgbgk_batch_default_params(dgbgk_batch_params* p);
@@ -240,12 +241,22 @@ void dgbgk_batch_default_params(dgbgk_batch_params* p);
 int dgbgk_batch_create(dgbgk_handle* const* cases, int ncases, const dgbgk_batch_params* p,
                        dgbgk_batch** out);
 
-/* Advances every case until its L2 residual falls to tol times its
+/* Advances every active case until its L2 residual falls to tol times its
  * reference (tol <= 0: no test) or it has run max_steps steps.
  * steps_done[ncases] and res_l2_last[ncases] (either may be NULL) receive
- * each case's step count and last L2 residual; the per-step histories stay
- * in the handles' devices and are not returned here. */
+ * each case's step count and last L2 residual (0 steps and 0.0 for a case
+ * that did not run); the per-step histories stay in the handles' devices
+ * and are not returned here.  A case that diverged (DGBGK_ENONFINITE) or
+ * whose device wait expired stays stopped, with that status, in later
+ * advances until its state is set again (dgbgk_set_state*, dgbgk_init_*,
+ * dgbgk_copy_state, dgbgk_extrapolate).  If a handle was changed on its own
+ * in a way that moved its device buffers (a longer dgbgk_advance, another
+ * batch's tile shape), the batch rebuilds its case table first. */
 int dgbgk_batch_advance(dgbgk_batch* b, int max_steps, double tol, int* steps_done, double* res_l2_last);
+
+/* active[ncases]: 0 leaves case i out of the following advances (0 steps,
+ * its state untouched), non-zero takes it back; every case starts active. */
+int dgbgk_batch_set_active(dgbgk_batch* b, const int* active);
 
 /* status[ncases]: each case's result of the last dgbgk_batch_advance()
  * (DGBGK_OK, DGBGK_ENONFINITE for a case that diverged and stopped, ...);

@@ -102,3 +102,109 @@ def test_batch_with_partial_accommodation_equals_cases_alone():
     Batch(batched, tune_steps=1).advance(5)
     for s, t in zip(batched, alone):
         assert rel_l2(s.get_state(), t.get_state()) <= 1e-13
+
+
+def stopping_cases():
+    """Eight cases of different meshes and velocity grids; the first (the
+    zero-gradient-sided channel at Kn = 1) diverges within a few hundred
+    steps, the scheme's stability limit, and stops while the others run."""
+    return [
+        channel_case(-5, 15, -5, 5, 40, 20, 8, 16, mach=2.0, kn=1.0, obstacle_side=1.0),
+        cavity_case(8, 8, 16, mach=0.3, kn=0.1),
+        channel_case(-2.0, 4.0, -2.0, 2.0, 24, 16, 5, 7, mach=2.0, kn=0.05, obstacle_side=1.0),
+        cavity_case(12, 6, 20, mach=0.8, kn=0.02, seed=3),
+        cavity_case(16, 8, 24, mach=0.5, kn=0.05, seed=5),
+        channel_case(-2.0, 4.0, -2.0, 2.0, 30, 20, 12, 12, mach=2.0, kn=0.05, obstacle_side=1.0),
+        cavity_case(10, 10, 10, mach=0.2, kn=0.3, seed=7),
+        cavity_case(20, 4, 36, mach=0.9, kn=0.5, seed=9),
+    ]
+
+
+SHAPES = [(eb, upc, rows) for eb in (64, 128) for upc in (2, 4, 8, 16) for rows in (1, 2, 4)]
+
+
+def test_every_batch_shape_with_a_case_stopping_early():
+    # every candidate tile shape (elements per CTA x units per CTA x moment
+    # rows), forced, on eight FP32 cases of which one diverges and stops
+    # while the others go on: each case's state (and the diverging case's
+    # step count) equals the case run alone.  This is the long heterogeneous
+    # march in which finished cases' work units are skipped.
+    from dgbgk._lib import DGBGK_ENONFINITE
+    cases = stopping_cases()
+    n = 700  # the first case's state turns non-finite near step 480 (oracle: between 450 and 500)
+    alone = [started(c, 32) for c in cases]
+    bad_steps = None
+    for k, s in enumerate(alone):
+        if k == 0:
+            r = s.advance(n, raise_on_error=False)
+            assert r["rc"] == DGBGK_ENONFINITE and r["steps"] < n
+            bad_steps = r["steps"]
+        else:
+            assert s.advance(n)["steps"] == n
+    states = [s.get_state() for s in alone[1:]]
+    for s in alone:
+        s.close()
+    for eb, upc, rows in SHAPES:
+        batched = [started(c, 32) for c in cases]
+        b = Batch(batched, tile_elems=eb, units_per_cta=upc, moment_rows=rows, tune_steps=1)
+        assert b.shape_record() == {"tile_elems": eb, "units_per_cta": upc, "moment_rows": rows}
+        r = b.advance(n, raise_on_error=False)
+        assert r["status"][0] == DGBGK_ENONFINITE and r["steps"][0] == bad_steps, (eb, upc, rows)
+        assert (r["status"][1:] == 0).all() and (r["steps"][1:] == n).all(), (eb, upc, rows)
+        for s, ref in zip(batched[1:], states):
+            assert rel_l2(s.get_state(), ref) <= 1e-5, (eb, upc, rows)
+        b.close()
+        for s in batched:
+            s.close()
+
+
+def test_batch_leaves_inactive_and_diverged_cases_alone():
+    # dgbgk_batch_set_active: an inactive case runs no step and keeps its
+    # state; a diverged case stays stopped, with its status, until its state
+    # is set again, and then runs like a fresh case
+    from dgbgk._lib import DgbgkError, DGBGK_ENONFINITE
+    cases = stopping_cases()[:3]
+    ss = [started(c, 32) for c in cases]
+    b = Batch(ss, tune_steps=1)
+    r = b.advance(700, raise_on_error=False)
+    assert r["status"][0] == DGBGK_ENONFINITE
+    kept = ss[2].get_state()
+    b.set_active([True, True, False])
+    with pytest.raises(DgbgkError) as e:
+        b.advance(10)
+    assert e.value.code == DGBGK_ENONFINITE
+    st = b.advance(10, raise_on_error=False)
+    assert list(st["steps"]) == [0, 10, 0] and list(st["status"]) == [DGBGK_ENONFINITE, 0, 0]
+    assert np.array_equal(ss[2].get_state(), kept)
+    # a new state lets the diverged case run again, like a fresh handle
+    ss[0].init_case()
+    b.set_active([True, False, False])
+    r0 = b.advance(5)
+    assert list(r0["steps"]) == [5, 0, 0] and list(r0["status"]) == [0, 0, 0]
+    fresh = started(cases[0], 32)
+    fresh.advance(5)
+    assert rel_l2(ss[0].get_state(), fresh.get_state()) <= 1e-6
+    b.close()
+    for s in ss + [fresh]:
+        s.close()
+
+
+def test_batch_rebuilds_its_table_after_a_case_moves_its_buffers():
+    # a case advanced alone for more steps than its history holds gets new
+    # device buffers; the batch must notice before its next launch
+    cases = stopping_cases()[1:4]
+    ss = [started(c, 64) for c in cases]
+    b = Batch(ss, tune_steps=1)
+    b.advance(3)
+    ss[1].advance(3000)              # grows that handle's history buffers
+    alone = [started(c, 64) for c in cases]
+    for s, n in zip(alone, (3, 3003, 3)):
+        s.advance(n)
+    b.advance(4)
+    for s in alone:
+        s.advance(4)
+    for s, t in zip(ss, alone):
+        assert rel_l2(s.get_state(), t.get_state()) <= 1e-12
+    b.close()
+    for s in ss + alone:
+        s.close()

@@ -12,7 +12,7 @@ import numpy as np
 import pytest
 
 from dgbgk import Batch, Solver, channel_case
-from dgbgk._lib import DGBGK_ENONFINITE
+from dgbgk._lib import DGBGK_ENONFINITE, DgbgkError
 from dgbgk.study import FAMILY, WarmStart, cold_reference, draw_cases, generate, nodal_fields, rel_fields
 from helpers import rel_l2
 
@@ -89,10 +89,28 @@ def test_batch_reports_a_diverging_case_and_finishes_the_rest():
     alone.init_case()
     alone.advance(1500)
     assert rel_l2(ss[1].get_state(), alone.get_state()) <= 1e-6
-    with pytest.raises(Exception):
+    # the diverged case stays stopped with its status; the advance reports
+    # it and runs the cavity on
+    with pytest.raises(DgbgkError) as e:
         b.advance(10)
+    assert e.value.code == DGBGK_ENONFINITE
+    assert list(b.advance(10, raise_on_error=False)["steps"]) == [0, 10]
     b.close()
-    alone.close()
+    for s in ss + [alone]:
+        s.close()
+    # the context is healthy: a fresh handle steps and matches the oracle
+    from pyoracle import Oracle
+    from dgbgk import node_scale
+    s = Solver.from_case(good, precision=64)
+    s.init_case()
+    s.advance(3)
+    o = Oracle.from_case(good, prec=64)
+    i = good.init
+    o.inicon2(i["T1"], i["P1"], i["U0"], i["V0"])
+    o.set_state(o.get_state() * node_scale(good)[:, None, :])
+    o.advance(3)
+    assert rel_l2(s.get_state(), o.get_state()) <= 1e-10
+    s.close()
 
 
 def test_trained_network_gains_over_the_cold_start():

@@ -38,12 +38,26 @@ class FakeCase:
 
 
 class FakeBatch:
+    """The library's batch semantics: cases left out by set_active, and
+    cases stopped by a divergence, run no step and keep their status."""
+
     def __init__(self, cases):
         self.cases = cases
+        self.active = np.ones(len(cases), dtype=bool)
+        self.stopped = np.zeros(len(cases), dtype=bool)
+        self.steps_run = np.zeros(len(cases), dtype=np.int64)
+
+    def set_active(self, active):
+        self.active = np.asarray(active, dtype=bool).copy()
 
     def advance(self, k, tol=0.0, raise_on_error=False):
         steps, last, status = [], [], []
-        for c in self.cases:
+        for i, c in enumerate(self.cases):
+            if not self.active[i] or self.stopped[i]:
+                steps.append(0)
+                last.append(0.0)
+                status.append(DGBGK_ENONFINITE if (self.active[i] and self.stopped[i]) else 0)
+                continue
             n, r, st = 0, np.inf, 0
             for _ in range(k):
                 c.step += 1
@@ -51,9 +65,11 @@ class FakeBatch:
                 r = c.res(c.step)
                 if not np.isfinite(r):
                     st = DGBGK_ENONFINITE
+                    self.stopped[i] = True
                     break
                 if tol > 0 and r <= tol:
                     break
+            self.steps_run[i] += n
             steps.append(n)
             last.append(r * c.ref)
             status.append(st)
@@ -68,10 +84,18 @@ def test_march_batch_stops_at_tolerance_plateau_and_divergence():
     plateau = FakeCase(lambda k: max(10 ** (-k / 500), 2e-6))      # FP32 rounding plateau
     bad = FakeCase(lambda k: np.nan if k > 1500 else 1.0)
     cases = [fast, plateau, bad]
-    steps, rel, status, _ = march_batch(FakeBatch(cases), cases, 1e-8, 60000)
+    b = FakeBatch(cases)
+    steps, rel, status, _ = march_batch(b, cases, 1e-8, 60000)
     assert steps[0] == 4000 and rel[0] <= 1e-8
     assert status[1] == 0 and abs(rel[1] - 2e-6) < 1e-12 and steps[1] < 6000
     assert status[2] == DGBGK_ENONFINITE
+    # finished cases are left out of later chunks: the diverged case ran
+    # 1501 steps (its last one non-finite) and the converged ones no step
+    # past their stop
+    assert b.steps_run[2] == 1501 and steps[2] == 1501
+    assert b.steps_run[0] == 4000 and b.steps_run[1] == steps[1]
+    # and the batch is handed back with every case active
+    assert b.active.all()
 
 
 def test_rre_driver_cycles_and_guard():

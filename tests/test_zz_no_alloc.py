@@ -15,7 +15,6 @@ import pytest
 
 from dgbgk import Solver, cavity_case
 from dgbgk._lib import DGBGK_EINVAL, check, lib, ptr
-from helpers import rel_l2
 
 pytestmark = pytest.mark.gpu
 
@@ -34,17 +33,19 @@ def test_noalloc_macros_match_allocating_entry_point_twice():
     s = Solver.from_case(cavity_case(8, 8, 16, mach=0.3, kn=0.1))
     s.init_case()
     s.advance(3)
+    # both entry points run the same moment and nodal-gather kernels on the
+    # same state, so their fields agree bit for bit (a stale or half-written
+    # scratch array would show here)
     for call in range(2):  # two calls in a row share the static array
         a = noalloc_macros(s)
         b = s.macros()
         for k in KEYS:
-            scale = 1.0 if k in ("u", "v") else 0.0  # velocities on the thermal-speed scale
-            assert rel_l2(a[k], b[k], scale) <= 1e-13, (call, k)
+            assert np.array_equal(a[k], b[k]), (call, k)
     s.advance(2)
     a = noalloc_macros(s)
     b = s.macros()
     for k in KEYS:
-        assert rel_l2(a[k], b[k], 1.0 if k in ("u", "v") else 0.0) <= 1e-13, k
+        assert np.array_equal(a[k], b[k]), k
 
 
 def test_noalloc_rejects_meshes_above_the_limit():

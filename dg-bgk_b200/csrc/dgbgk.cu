@@ -944,7 +944,7 @@ template <class T> struct Impl : ImplBase {
 
   int init_uniform(double t1, double p1, double u0, double v0, const double* scale) override {
     CK(cudaSetDevice(device));
-    // INICON2 (src/inicon2.f90:216-251) evaluated per velocity in double
+    // INICON2 (src/inicon2.f90:120-174) evaluated per velocity in double
     const double PI = 3.1416, NA = 6.022e26;
     const double rho1 = (p1 * 100000.0) / (pl.rgas * t1);
     const double n1 = rho1 * NA / pl.M;

@@ -5,7 +5,7 @@
 // Follows src/spectralbgk.f90 (the &Input namelist with its defaults, the
 // Lobatto file, the .plt mesh and the FILE.OUT echo), DG_LIN_CONVEC's setup
 // (src/dg_lin_convec.f90:70-120: GETSID .. GETNOR, INICON2) and ADVNCE's
-// output (src/advnce.f90:86-169, 274-329): RESULTS1.RES / RESULTS2.RES
+// output (src/advnce.f90:103-120, 154-175, 403-435): RESULTS1.RES / RESULTS2.RES
 // blocks at step 0, every 1000 steps and after the loop, and one
 // RESIDUAL.RES line per step (log of max|DELUN| over the first step's, with
 // GETFOR's lift and drag when FORCEOUT != 0, src/getfor.f90).  Files are

@@ -3,8 +3,8 @@
 // One step (src/advnce.f90:220-400) is four launches on one stream (five
 // with ALPHA < 1: k_wspec after the sweep):
 //   k_moments : MACROS passes 1+2 (src/macros.f90:80-154) fused with COMPMU
-//               (src/compmu.f90:242-290) and the GTEQNF parameters
-//               (src/gteqnf.f90:315-326).  Persistent warps take R whole
+//               (src/compmu.f90:36-97) and the GTEQNF parameters
+//               (src/gteqnf.f90:26-40).  Persistent warps take R whole
 //               velocity rows of f at a time (32/R lanes per row) from a
 //               per-warp ring of stages filled by 1-D bulk copies, so f is
 //               read from HBM once for both passes; every access is a
@@ -236,7 +236,7 @@ template <> struct RowMath<double> {
       const double q0 = dx0 * dx0 + dy0 * dy0, q1 = dx1 * dx1 + dy1 * dy1;
       const double a0 = w.x * x.x, a1 = w.y * x.y;
       sp = fma(0.5 * q0, a0, fma(0.5 * q1, a1, sp));                // src/macros.f90:144-148
-      sc = fma(sqrt_newton(q0), a0, fma(sqrt_newton(q1), a1, sc));  // src/compmu.f90:264-267
+      sc = fma(sqrt_newton(q0), a0, fma(sqrt_newton(q1), a1, sc));  // src/compmu.f90:71-74
     }
   }
 };
@@ -403,7 +403,7 @@ __global__ void __launch_bounds__(ONE ? 640 : 512, 1)
       const double mu = sqrt(2.0) * ct * C.sigt * nd;
       const int e = node / 3, i = node - 3 * (node / 3);
       ElemRec<T>& en = C.rec[e];
-      if (ps >= TINY_D) {  // GTEQNF (src/gteqnf.f90:317-326)
+      if (ps >= TINY_D) {  // GTEQNF (src/gteqnf.f90:28-37)
         const double rho = C.MM * nd;
         const double b2 = rho / (2 * ps);
         en.A[i] = (T)(nd * (b2 / PI_D));
@@ -615,7 +615,7 @@ template <class T> __device__ __forceinline__ void vst(void* p, const typename V
 }
 
 // Phase 1 of the sweep on chunk c of an element's three rows (tile rows
-// r0 .. r0+2): NFO (GTEQNF, src/gteqnf.f90:324-326) and UMEAN =
+// r0 .. r0+2): NFO (GTEQNF, src/gteqnf.f90:35-37) and UMEAN =
 // 0.5*DTE*(div F - 1/3 sum_i MU_i (NFO_i - f_i)) with div F = sum_i
 // (N_i,x cx + N_i,y cy) f_i (GETELC, src/getelc.f90:54-83).  The rows are
 // overwritten in place with g = f - UMEAN, the value every edge flux and the
@@ -1466,7 +1466,7 @@ __global__ void k_from_internal(const T* __restrict__ src, S* __restrict__ dst, 
     for (int v = threadIdx.x; v < V; v += blockDim.x) d[(size_t)v * 3 + i] = (S)src[(en * 3 + i) * Vp + v];
 }
 
-// INICON2 (src/inicon2.f90:231-262) times an optional per-DG-node scale.
+// INICON2 (src/inicon2.f90:143-174) times an optional per-DG-node scale.
 template <class T>
 __global__ void k_init_uniform(T* __restrict__ f, const double* __restrict__ g, const double* __restrict__ scale,
                                double n1, int V, int Vp, size_t ndg) {

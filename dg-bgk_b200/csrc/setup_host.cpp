@@ -64,7 +64,7 @@ struct SideRec {
   int left, right;
 };
 
-// The reference side table (src/getsid.f90:14-266): sides are created while
+// The reference side table (src/getsid.f90:1-216): sides are created while
 // scanning points in ascending order; a side (P, Q) with Q > P is created by
 // the first element around P (ascending element order) that contains it.
 // The element in which Q follows P in local order goes to ISIDE(3), the

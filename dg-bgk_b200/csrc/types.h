@@ -38,11 +38,11 @@ template <class T> struct alignas(16) ElemEdge {
 // needs; the moment kernel rewrites the node parameters every step.
 template <class T> struct alignas(16) ElemRec {
   T gx[3], gy[3];  // shape-function gradients GEOME(1:3), GEOME(4:6)
-  T A[3];    // DISND*BETA2/PI   (0 where DISPS < 1e-20: NFO = 0, src/gteqnf.f90:321)
+  T A[3];    // DISND*BETA2/PI   (0 where DISPS < 1e-20: NFO = 0, src/gteqnf.f90:32)
   T ex[3];   // exponent coefficient of NFO: -BETA2 (FP64), -BETA2*log2(e) (FP32, for 2^x)
   T ux[3];   // DISUX
   T uy[3];   // DISUY
-  T mu[3];   // collision frequency MU (src/compmu.f90:284-285)
+  T mu[3];   // collision frequency MU (src/compmu.f90:90-92)
   T area;    // 0.5 * GEOME(7)   (src/getelc.f90:44)
   T mm[3];   // MMAT (IMMAT = 1) or CMMAT row sums (IMMAT = 0)
   int bside[3];  // boundary side index of each wall edge (kind 3), else -1

@@ -5,8 +5,8 @@
  * The library replaces the reference time step ADVNCE (src/advnce.f90:3-25,
  * called once from src/dg_lin_convec.f90:185-206) and the output gather
  * GETMAC (src/getmac.f90:3-127).  A host written in any language binds these
- * entry points; the Fortran ISO_C_BINDING binding that DG_LIN_CONVEC would
- * use is given in INTEGRATION.md.
+ * entry points; a Fortran host binds them through ISO_C_BINDING interfaces
+ * with the same argument lists (BIND(C), VALUE for the scalars).
  *
  * Conventions
  *  - Every array argument is caller-owned host memory and is copied in or
@@ -47,7 +47,7 @@ typedef struct dgbgk_mesh {
   const int* intma;     /* INTMA(3,NELEM)            src/gtinpt.f90:27-29  */
   const double* coord;  /* COORD(2,NPOIN)            src/gtinpt.f90:36-38  */
   const int* bsido;     /* BSIDO(6,NBOUN)            src/gtinpt.f90:48-50  */
-  const int* iside;     /* ISIDE(8,NSIDE)            src/getsid.f90:14-266 */
+  const int* iside;     /* ISIDE(8,NSIDE)            src/getsid.f90:1-216 */
   const double* nx;     /* NX(NSIDE)                 src/normal.f90:24-33  */
   const double* ny;     /* NY(NSIDE)                                       */
   const double* el;     /* EL(NSIDE)                                       */
@@ -91,7 +91,7 @@ typedef struct dgbgk_params {
  * src/spectralbgk.f90:116-147 plus precision 64. */
 void dgbgk_default_params(dgbgk_params* p);
 
-/* Host-side setup: GETSID (src/getsid.f90:14-266), NORMAL
+/* Host-side setup: GETSID (src/getsid.f90:1-216), NORMAL
  * (src/normal.f90:24-33), GETGEO (src/getgeo.f90:22-59), GETLEN
  * (src/getlen.f90:17-26), GETMAT (src/getmat.f90:17-40) or CONMAT
  * (src/conmat.f90:17-41) and GETNOR (src/getnor.f90:21-31) from INTMA, COORD
@@ -119,7 +119,7 @@ int dgbgk_get_state(dgbgk_handle* h, double* disnf);
 int dgbgk_set_state_f32(dgbgk_handle* h, const float* disnf);
 int dgbgk_get_state_f32(dgbgk_handle* h, float* disnf);
 
-/* INICON2 (src/inicon2.f90:208-262): the uniform Maxwellian at T1, P1 [bar],
+/* INICON2 (src/inicon2.f90:116-180): the uniform Maxwellian at T1, P1 [bar],
  * (U0, V0), optionally scaled per DG node by node_scale(3,NELEM) (NULL = 1;
  * the seeded density perturbation of the benchmark cases).  Built on the
  * device. */
@@ -173,7 +173,7 @@ int dgbgk_get_macros(dgbgk_handle* h, double* nd, double* rho, double* u, double
 
 /* Discontinuous per-DG-node fields of the current state (each (3,NELEM)):
  * DISND, DISUX, DISUY, DISPS (src/macros.f90:131-164) and MU
- * (src/compmu.f90:279-290).  Any pointer may be NULL. */
+ * (src/compmu.f90:86-97).  Any pointer may be NULL. */
 int dgbgk_get_node_fields(dgbgk_handle* h, double* disnd, double* disux, double* disuy,
                           double* disps, double* mu);
 

@@ -331,7 +331,7 @@ template <class R> void alotim(Case<R>& c) {
   c.DTEc = DTE;
 }
 
-// src/inicon2.f90:208-262 (uniform Maxwellian initial condition)
+// src/inicon2.f90:116-180 (uniform Maxwellian initial condition)
 template <class R> void inicon2(Case<R>& c, R T1, R P1, R U0, R V0) {
   const R PI = K<R>::PI(), NA = K<R>::NA();
   const R E5 = (R)100000;

@@ -1,7 +1,8 @@
 """Regenerates the golden fixtures of tests/golden/ from the reference tree.
 
-Run in the build container (the reference is not present on GPU machines):
-    python tests/golden/make_fixtures.py /root/reference
+Run where the reference tree is present (it is not on GPU machines), with
+the reference's root directory as the one argument:
+    python tests/golden/make_fixtures.py <reference-root>
 Writes:
   * Lobatto40.txt, Lobatto10.txt -- the reference's velocity-quadrature files
     (tc/tc1/Lobatto40.txt, tc/tc4/Lobatto10.txt), copied verbatim;
@@ -53,4 +54,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_fixtures.py <reference-root>")
+    main(sys.argv[1])

@@ -108,13 +108,15 @@ def stopping_cases():
     """Eight cases of different meshes and velocity grids; the first (the
     zero-gradient-sided channel at Kn = 1) diverges within a few hundred
     steps, the scheme's stability limit, and stops while the others run."""
+    # the other seven stay finite for at least 1000 steps (checked with the
+    # FP32 oracle)
     return [
         channel_case(-5, 15, -5, 5, 40, 20, 8, 16, mach=2.0, kn=1.0, obstacle_side=1.0),
         cavity_case(8, 8, 16, mach=0.3, kn=0.1),
-        channel_case(-2.0, 4.0, -2.0, 2.0, 24, 16, 5, 7, mach=2.0, kn=0.05, obstacle_side=1.0),
+        channel_case(-2.0, 4.0, -3.0, 3.0, 30, 30, 12, 24, mach=2.5, kn=0.07, obstacle_side=1.0, sides="freestream"),
         cavity_case(12, 6, 20, mach=0.8, kn=0.02, seed=3),
         cavity_case(16, 8, 24, mach=0.5, kn=0.05, seed=5),
-        channel_case(-2.0, 4.0, -2.0, 2.0, 30, 20, 12, 12, mach=2.0, kn=0.05, obstacle_side=1.0),
+        cavity_case(12, 8, 16, mach=0.6, kn=0.05, seed=5),
         cavity_case(10, 10, 10, mach=0.2, kn=0.3, seed=7),
         cavity_case(20, 4, 36, mach=0.9, kn=0.5, seed=9),
     ]

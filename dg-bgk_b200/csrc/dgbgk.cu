@@ -621,20 +621,31 @@ template <class T> struct Impl : ImplBase {
       std::memset((void*)r.data(), 0, r.size() * sizeof(ElemRec<T>));
       for (int e = 0; e < pl.E; ++e) {
         const auto& g = pl.geo[e];
-        int flags = g.inflow & 7;
+        int flags = g.inflow & 7, interior = 0;
         for (int k = 0; k < 3; ++k) {
           r[e].gx[k] = (T)g.gx[k];
           r[e].gy[k] = (T)g.gy[k];
           r[e].mm[k] = (T)g.mm[k];
           const size_t i = 3 * (size_t)e + k;
-          r[e].edge[k].nx = (T)pl.edge[i].nx;
-          r[e].edge[k].ny = (T)pl.edge[i].ny;
-          r[e].edge[k].alen = (T)pl.edge[i].alen;
-          r[e].edge[k].info = edge_info(pl, i, e % eb);
-          const bool wall = (pl.edge[i].low & 3) == 3;
-          r[e].bside[k] = wall ? pl.edge[i].bside : -1;
+          const PlanEdge& pe = pl.edge[i];
+          r[e].edge[k].anx = (T)(pe.alen * pe.nx);
+          r[e].edge[k].any = (T)(pe.alen * pe.ny);
+          // the flux source's rows: the neighbour's (its slot and local
+          // nodes) across an interior side, the element's own otherwise
+          const int inf = edge_info(pl, i, e % eb);
+          const int slot = inf >> 8, kind = inf & 3;
+          r[e].edge[k].offp = tile_row_off(3 * slot + ((inf >> 3) & 3));
+          r[e].edge[k].offq = tile_row_off(3 * slot + ((inf >> 5) & 3));
+          if (kind == 0 || kind == 2) flags |= FLAG_FLUX0 << k;
+          if (kind == 0) ++interior;
+          const bool wall = kind == 3;
+          r[e].bside[k] = wall ? pe.bside : -1;
           if (wall) flags |= 8 << k;
         }
+        if (interior == 3) flags |= FLAG_INTERIOR;
+        const int j = e % eb;
+        r[e].own01 = tile_row_off(3 * j) | (tile_row_off(3 * j + 1) << 16);
+        r[e].own2 = tile_row_off(3 * j + 2);
         r[e].area = (T)g.area;
         r[e].flags = flags;
         r[e].wslot = pl.spec ? pl.wslot[e] : -1;

@@ -403,17 +403,29 @@ __global__ void __launch_bounds__(ONE ? 640 : 512, 1)
       const double mu = sqrt(2.0) * ct * C.sigt * nd;
       const int e = node / 3, i = node - 3 * (node / 3);
       ElemRec<T>& en = C.rec[e];
-      if (ps >= TINY_D) {  // GTEQNF (src/gteqnf.f90:28-37)
+      // GTEQNF's parameters (src/gteqnf.f90:28-37); FP64 in the expanded
+      // exponent form of the sweep (ElemRec)
+      if (ps >= TINY_D) {
         const double rho = C.MM * nd;
         const double b2 = rho / (2 * ps);
-        en.A[i] = (T)(nd * (b2 / PI_D));
-        en.ex[i] = (T)(sizeof(T) == 4 ? -b2 * LOG2E_D : -b2);
+        const double a = nd * (b2 / PI_D);
+        if (sizeof(T) == 4) {
+          en.A[i] = (T)a;
+          en.ex[i] = (T)(-b2 * LOG2E_D);
+          en.ux[i] = (T)ux;
+          en.uy[i] = (T)uy;
+        } else {
+          en.A[i] = (T)(log(a) - b2 * (ux * ux + uy * uy));
+          en.ex[i] = (T)(-b2);
+          en.ux[i] = (T)(2.0 * b2 * ux);
+          en.uy[i] = (T)(2.0 * b2 * uy);
+        }
       } else {
-        en.A[i] = (T)0;
+        en.A[i] = (T)(sizeof(T) == 4 ? 0.0 : -INFINITY);
         en.ex[i] = (T)0;
+        en.ux[i] = (T)(sizeof(T) == 4 ? ux : 0.0);
+        en.uy[i] = (T)(sizeof(T) == 4 ? uy : 0.0);
       }
-      en.ux[i] = (T)ux;
-      en.uy[i] = (T)uy;
       en.mu[i] = (T)mu;
       C.nraw[node] = s0;
       C.disux[node] = ux;
@@ -511,6 +523,9 @@ template <class T> struct SweepGeo {
   static constexpr int HW = (REC_HEAD_VALUES * (int)sizeof(T) + 15) / 16;        // head words
   static constexpr int HR = 16 * (HW | 1);  // halo head pitch (odd number of words)
   static constexpr int TPU_MAX = 16;
+  // velocity tables staged per unit: cx, cy, NFINF (and |c|^2 for the FP64
+  // exponent)
+  static constexpr int NTAB = sizeof(T) == 8 ? 4 : 3;
   // one tile buffer, 1024-byte aligned
   static constexpr size_t tile_bytes(int EB, int max_halo) {
     return ((size_t)3 * (EB + max_halo) * 64 + 1023) / 1024 * 1024;
@@ -519,14 +534,10 @@ template <class T> struct SweepGeo {
   // velocity tables cx, cy, NFINF [3][TPU_MAX * VT], halo element list
   static constexpr size_t smem(int EB, int max_halo) {
     return 1024 + 2 * tile_bytes(EB, max_halo) + (size_t)EB * sizeof(ElemRec<T>) + (size_t)max_halo * HR +
-           3 * (size_t)TPU_MAX * VT * sizeof(T) + ((size_t)max_halo * 4 + 15) / 16 * 16;
+           NTAB * (size_t)TPU_MAX * VT * sizeof(T) + ((size_t)3 * max_halo * 4 + 15) / 16 * 16;
   }
 };
 
-// Byte offset of 16-byte chunk c of row r in a tile.
-__device__ __forceinline__ unsigned tile_off(int r, int c) {
-  return (unsigned)(r * 64 + 16 * (c ^ ((r >> 1) & 3)));
-}
 
 // A tensor map read from global memory (the batch's case table, written by
 // a host copy) must be acquired by the tensormap proxy before a thread uses
@@ -614,26 +625,25 @@ template <class T> __device__ __forceinline__ void vst(void* p, const typename V
   *reinterpret_cast<typename Vec<T>::type*>(p) = v;
 }
 
-// Phase 1 of the sweep on chunk c of an element's three rows (tile rows
-// r0 .. r0+2): NFO (GTEQNF, src/gteqnf.f90:35-37) and UMEAN =
-// 0.5*DTE*(div F - 1/3 sum_i MU_i (NFO_i - f_i)) with div F = sum_i
+// Phase 1 of the sweep on one 16-byte chunk of an element's three rows
+// (tile byte offsets ro[0..2]): NFO (GTEQNF, src/gteqnf.f90:35-37) and
+// UMEAN = 0.5*DTE*(div F - 1/3 sum_i MU_i (NFO_i - f_i)) with div F = sum_i
 // (N_i,x cx + N_i,y cy) f_i (GETELC, src/getelc.f90:54-83).  The rows are
 // overwritten in place with g = f - UMEAN, the value every edge flux and the
 // volume term of this element use (src/getelc.f90:87-117,
-// src/edgflxopt.f90:95-125); NFO and UMEAN are returned.
+// src/edgflxopt.f90:95-125); NFO and UMEAN are returned.  FP32: NFO =
+// A*2^(ex*|c-u|^2) with the SFU's 2^x; FP64: NFO = exp(a0 + a1*cx + a2*cy +
+// ex*|c|^2) (the exponent expanded, three FMAs; c2 = |c|^2 per velocity).
 template <class T>
-__device__ __forceinline__ void sweep_p1(const ElemRec<T>& r, const double* etab, unsigned char* tl, int r0, int c,
-                                         const typename Vec<T>::type& cxv, const typename Vec<T>::type& cyv, T dth,
+__device__ __forceinline__ void sweep_p1(const ElemRec<T>& r, const double* etab, unsigned char* tl,
+                                         const unsigned (&ro)[3], const typename Vec<T>::type& cxv,
+                                         const typename Vec<T>::type& cyv, const typename Vec<T>::type& c2v, T dth,
                                          T dth3, typename Vec<T>::type (&q)[3], typename Vec<T>::type& u) {
   using VO = Vec<T>;
   constexpr int W = SweepGeo<T>::W;
-  unsigned char* row[3];
   typename VO::type f[3];
 #pragma unroll
-  for (int i = 0; i < 3; ++i) {
-    row[i] = tl + tile_off(r0 + i, c);
-    f[i] = vld<T>(row[i]);
-  }
+  for (int i = 0; i < 3; ++i) f[i] = vld<T>(tl + ro[i]);
 #pragma unroll
   for (int w = 0; w < W; ++w) {
     const T cx = VO::get(cxv, w), cy = VO::get(cyv, w);
@@ -643,8 +653,13 @@ __device__ __forceinline__ void sweep_p1(const ElemRec<T>& r, const double* etab
     T coll = (T)0;
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
-      const T dx = r.ux[i] - cx, dy = r.uy[i] - cy;
-      const T qi = r.A[i] * nfo_exp<T>(r.ex[i] * (dx * dx + dy * dy), etab);
+      T qi;
+      if constexpr (sizeof(T) == 8) {
+        qi = exp_tang(fma(r.ux[i], cx, fma(r.uy[i], cy, fma(r.ex[i], VO::get(c2v, w), r.A[i]))), etab);
+      } else {
+        const T dx = r.ux[i] - cx, dy = r.uy[i] - cy;
+        qi = r.A[i] * nfo_exp<T>(r.ex[i] * (dx * dx + dy * dy), etab);
+      }
       VO::set(q[i], w, qi);
       coll += r.mu[i] * (qi - VO::get(f[i], w));
     }
@@ -654,115 +669,19 @@ __device__ __forceinline__ void sweep_p1(const ElemRec<T>& r, const double* etab
     for (int i = 0; i < 3; ++i) VO::set(f[i], w, VO::get(f[i], w) - um);
   }
 #pragma unroll
-  for (int i = 0; i < 3; ++i) vst<T>(row[i], f[i]);
+  for (int i = 0; i < 3; ++i) vst<T>(tl + ro[i], f[i]);
 }
 
-// FP32 phase 1 on packed pairs of velocities (fma.rn.f32x2, mul/add.f32x2:
-// one instruction per two velocities of an element, the element's
-// coefficients broadcast to both halves), the same operations per value as
-// the generic sweep_p1.  Built only with DGBGK_SWEEP_PACKED32 >= 1: it
-// compiles to the same 128 registers without spills in the single-case
-// sweep, and is kept out of the default build until measured on the GPU.
-#ifndef DGBGK_SWEEP_PACKED32
-#define DGBGK_SWEEP_PACKED32 0
-#endif
-#if DGBGK_SWEEP_PACKED32
-__device__ __forceinline__ float2 bc2(float x) { return make_float2(x, x); }
-template <>
-__device__ __forceinline__ void sweep_p1<float>(const ElemRec<float>& r, const double* etab, unsigned char* tl, int r0,
-                                                int c, const float4& cxv, const float4& cyv, float dth, float dth3,
-                                                float4 (&q)[3], float4& u) {
-  unsigned char* row[3];
-  float4 f4[3];
-#pragma unroll
-  for (int i = 0; i < 3; ++i) {
-    row[i] = tl + tile_off(r0 + i, c);
-    f4[i] = vld<float>(row[i]);
-  }
-  const float2 m1 = bc2(-1.0f);
-#pragma unroll
-  for (int h = 0; h < 2; ++h) {
-    const float2 cx = h ? make_float2(cxv.z, cxv.w) : make_float2(cxv.x, cxv.y);
-    const float2 cy = h ? make_float2(cyv.z, cyv.w) : make_float2(cyv.x, cyv.y);
-    float2 f[3];
-#pragma unroll
-    for (int i = 0; i < 3; ++i) f[i] = h ? make_float2(f4[i].z, f4[i].w) : make_float2(f4[i].x, f4[i].y);
-    float2 sx = __fmul2_rn(bc2(r.gx[0]), f[0]);
-    sx = __ffma2_rn(bc2(r.gx[1]), f[1], sx);
-    sx = __ffma2_rn(bc2(r.gx[2]), f[2], sx);
-    float2 sy = __fmul2_rn(bc2(r.gy[0]), f[0]);
-    sy = __ffma2_rn(bc2(r.gy[1]), f[1], sy);
-    sy = __ffma2_rn(bc2(r.gy[2]), f[2], sy);
-    float2 coll = bc2(0.0f);
-    float2 qq[3];
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-      const float2 dx = __ffma2_rn(cx, m1, bc2(r.ux[i]));
-      const float2 dy = __ffma2_rn(cy, m1, bc2(r.uy[i]));
-      const float2 arg = __fmul2_rn(bc2(r.ex[i]), __ffma2_rn(dx, dx, __fmul2_rn(dy, dy)));
-      qq[i] = __fmul2_rn(bc2(r.A[i]), make_float2(nfo_exp<float>(arg.x, etab), nfo_exp<float>(arg.y, etab)));
-      coll = __ffma2_rn(bc2(r.mu[i]), __ffma2_rn(f[i], m1, qq[i]), coll);
-    }
-    float2 um = __fmul2_rn(bc2(dth), __ffma2_rn(sy, cy, __fmul2_rn(sx, cx)));
-    um = __ffma2_rn(bc2(-dth3), coll, um);
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-      const float2 g = __ffma2_rn(um, m1, f[i]);
-      if (h) { q[i].z = qq[i].x; q[i].w = qq[i].y; f4[i].z = g.x; f4[i].w = g.y; }
-      else { q[i].x = qq[i].x; q[i].y = qq[i].y; f4[i].x = g.x; f4[i].y = g.y; }
-    }
-    if (h) { u.z = um.x; u.w = um.y; } else { u.x = um.x; u.y = um.y; }
-  }
-#pragma unroll
-  for (int i = 0; i < 3; ++i) vst<float>(row[i], f4[i]);
+// max that keeps a NaN operand (max.NaN): the residual's "change the
+// unknown receives" must carry a non-finite update into the L2 sum
+__device__ __forceinline__ float fmax_nan(float a, float b) {
+  float r;
+  asm("max.NaN.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
+  return r;
 }
-
-#if DGBGK_SWEEP_PACKED32 >= 2
-// Volume and edge terms of one 16-byte chunk (four velocities) on packed
-// pairs: RHS_i = AREA/3 (N_i,x cx + N_i,y cy) sum(g) and the upwind edge
-// fluxes, the same operations per value as the generic loops of k_sweep;
-// the upwind choice stays per velocity.  Level 2 of DGBGK_SWEEP_PACKED32
-// (with it the single-case FP32 sweep spills 36 bytes at 128 registers).
-__device__ __forceinline__ void sweep_rhs_packed(const ElemRec<float>& r, float area3, const float4& cxv,
-                                                 const float4& cyv, const float4 (&g)[3], const unsigned char* tl,
-                                                 const unsigned (&srcp)[3], const unsigned (&srcq)[3], unsigned cx16,
-                                                 const float (&anx)[3], const float (&any)[3], float (&rhs)[3][4]) {
-  const float2 m1 = bc2(-1.0f), two = bc2(2.0f);
-  auto pr = [](const float4& v, int h) { return h ? make_float2(v.z, v.w) : make_float2(v.x, v.y); };
-  float2 rr[2][3];
-#pragma unroll
-  for (int h = 0; h < 2; ++h) {
-    const float2 cx = pr(cxv, h), cy = pr(cyv, h);
-    const float2 s3 = __fmul2_rn(__fadd2_rn(__fadd2_rn(pr(g[0], h), pr(g[1], h)), pr(g[2], h)), bc2(area3));
-    rr[h][0] = __fmul2_rn(__ffma2_rn(bc2(r.gx[0]), cx, __fmul2_rn(bc2(r.gy[0]), cy)), s3);
-    rr[h][1] = __fmul2_rn(__ffma2_rn(bc2(r.gx[1]), cx, __fmul2_rn(bc2(r.gy[1]), cy)), s3);
-    rr[h][2] = __fmul2_rn(__fadd2_rn(rr[h][0], rr[h][1]), m1);
-  }
-#pragma unroll
-  for (int k2 = 0; k2 < 3; ++k2) {
-    const int p = k2, qn = (k2 + 1) % 3;
-    const float4 gp4 = vld<float>(tl + (srcp[k2] ^ cx16)), gq4 = vld<float>(tl + (srcq[k2] ^ cx16));
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const float2 as = __ffma2_rn(bc2(anx[k2]), pr(cxv, h), __fmul2_rn(bc2(any[k2]), pr(cyv, h)));
-      const float2 gp = pr(gp4, h), gq = pr(gq4, h), op = pr(g[p], h), oq = pr(g[qn], h);
-      const float2 up = make_float2(as.x > 0.0f ? op.x : gp.x, as.y > 0.0f ? op.y : gp.y);
-      const float2 uq = make_float2(as.x > 0.0f ? oq.x : gq.x, as.y > 0.0f ? oq.y : gq.y);
-      const float2 nas = __fmul2_rn(as, m1);
-      rr[h][p] = __ffma2_rn(nas, __ffma2_rn(two, up, uq), rr[h][p]);
-      rr[h][qn] = __ffma2_rn(nas, __ffma2_rn(two, uq, up), rr[h][qn]);
-    }
-  }
-#pragma unroll
-  for (int h = 0; h < 2; ++h)
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-      rhs[i][2 * h] = rr[h][i].x;
-      rhs[i][2 * h + 1] = rr[h][i].y;
-    }
+__device__ __forceinline__ double fmax_nan(double a, double b) {
+  return (a != a || b != b) ? a + b : fmax(a, b);
 }
-#endif  // DGBGK_SWEEP_PACKED32 >= 2
-#endif  // DGBGK_SWEEP_PACKED32
 
 // Persistent sweep kernel: EB block elements, TPE*EB threads.  Work units are
 // (block b, group of `tpu` velocity tiles) with b fastest, handed out in
@@ -822,9 +741,9 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : (E
   const size_t tile_bytes = G::tile_bytes(EB, a.max_halo);
   ElemRec<T>* const recs = reinterpret_cast<ElemRec<T>*>(base + 2 * tile_bytes);
   unsigned char* const hrec = reinterpret_cast<unsigned char*>(recs + EB);
-  T* const vtab = reinterpret_cast<T*>(hrec + (size_t)a.max_halo * HR);  // cx, cy, NFINF
+  T* const vtab = reinterpret_cast<T*>(hrec + (size_t)a.max_halo * HR);  // cx, cy, NFINF (, |c|^2)
   constexpr int UV = G::TPU_MAX * VT;
-  int* const hl = reinterpret_cast<int*>(vtab + 3 * UV);  // halo elements of the unit's block
+  int* const hrow = reinterpret_cast<int*>(vtab + G::NTAB * UV);  // f rows of the unit's halo, 3 per element
   const int j = tid % EB, hh = tid / EB;  // block element, and which of its TPE parts
   const T third = (T)(1.0 / 3.0);
   if (tid == 0) {
@@ -870,9 +789,8 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : (E
       const T dt = (T)dtd, dth = (T)(0.5 * dtd), dth3 = (T)(0.5 * dtd / 3.0);
       double rmax = 0.0, rsq = 0.0;
 
-      // unit prologue: block records and halo record heads (cp.async,
-      // completed with the first tile's group), the halo list and the
-      // velocity tables
+      // unit prologue: block records and halo record heads (cp.async, one
+      // group), the halo's f rows and the velocity tables
       {
         const uint4* src = reinterpret_cast<const uint4*>(C.rec + e0);
         for (int w = tid; w < nb * RW; w += NT) cp_async16(reinterpret_cast<uint4*>(recs) + w, src + w);
@@ -881,18 +799,24 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : (E
           const int s = w / HW, k = w - s * HW;
           cp_async16(hrec + (size_t)s * HR + 16 * k, reinterpret_cast<const uint4*>(C.rec + hlist[s]) + k);
         }
-        for (int s = tid; s < nh; s += NT) hl[s] = hlist[s];
+        cp_async_commit();
+        for (int s = tid; s < 3 * nh; s += NT) {
+          const int h = s / 3;
+          hrow[s] = hlist[h] * 3 + (s - 3 * h);
+        }
         const int v0 = vt0 * VT;
         for (int v = tid; v < ntl * VT; v += NT) {
-          vtab[v] = C.cx[v0 + v];
-          vtab[UV + v] = C.cy[v0 + v];
+          const T cx = C.cx[v0 + v], cy = C.cy[v0 + v];
+          vtab[v] = cx;
+          vtab[UV + v] = cy;
           vtab[2 * UV + v] = C.nfinf[v0 + v];
+          if (G::NTAB == 4) vtab[3 * UV + v] = cx * cx + cy * cy;
         }
       }
       // copies of tile vt into buffer bi: the block's rows (3*e0 ..) as NBOX
       // TMA boxes issued by thread 0 once the buffer's last box store has
-      // read it (rows past 3E read as zeros), the halo rows by cp.async, four
-      // threads per 64-byte row
+      // read it (rows past 3E read as zeros), the halo rows (tile rows 3*EB
+      // ..) by cp.async, four threads per 64-byte row
       auto issue = [&](int vt, int bi) {
         unsigned char* dst = base + (size_t)bi * tile_bytes;
         if (tid == 0) {
@@ -905,13 +829,14 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : (E
         }
         const T* src = C.f[cur] + (size_t)vt * VT;
         for (int w = tid; w < nh * 12; w += NT) {
-          const int h = w / 12, rr = w - 12 * h, i = rr >> 2, cq = rr & 3;
-          cp_async16(dst + tile_off(3 * (EB + h) + i, cq), src + ((size_t)hl[h] * 3 + i) * C.Vp + cq * W);
+          const int row = w >> 2, cq = w & 3;
+          cp_async16(dst + (tile_row_off(3 * EB + row) ^ (16u * cq)), src + (size_t)hrow[row] * C.Vp + cq * W);
         }
       };
-      __syncthreads();  // hl
+      __syncthreads();  // hrow, vtab
       issue(vt0, 0);
       cp_async_commit();
+      const unsigned hx = 16u * CPT * hh;  // the thread's first chunk, as an offset XOR
 
       for (int k = 0; k < ntl; ++k) {
         const int bi = k & 1;
@@ -935,7 +860,12 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : (E
         const T* vx = vtab + k * VT;
         const T* vy = vtab + UV + k * VT;
         const T* vn = vtab + 2 * UV + k * VT;
+        const T* vc2 = vtab + (G::NTAB - 1) * UV + k * VT;  // |c|^2 (FP64; unused in FP32)
 
+        // block element j's own rows at the thread's first chunk
+        unsigned own[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) own[i] = tile_row_off(3 * j + i) ^ hx;
         // ---- phase 1: block element j (chunks CPT*hh ..), then the halo
         // chunk by chunk
         VecT qr[CPT][3], ur[CPT];
@@ -944,14 +874,20 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : (E
 #pragma unroll
           for (int cc = 0; cc < CPT; ++cc) {
             const int cq = CPT * hh + cc;
-            sweep_p1<T>(r, etab, tl, 3 * j, cq, vld<T>(vx + cq * W), vld<T>(vy + cq * W), dth, dth3, qr[cc], ur[cc]);
+            const unsigned ro[3] = {own[0] ^ (16u * cc), own[1] ^ (16u * cc), own[2] ^ (16u * cc)};
+            sweep_p1<T>(r, etab, tl, ro, vld<T>(vx + cq * W), vld<T>(vy + cq * W), vld<T>(vc2 + cq * W), dth, dth3,
+                        qr[cc], ur[cc]);
           }
         }
         for (int w = tid; w < nh * NCH; w += NT) {
           const int hs = w >> 2, cq = w & 3;
           const ElemRec<T>& r = *reinterpret_cast<const ElemRec<T>*>(hrec + (size_t)hs * HR);
+          const int r0 = 3 * (EB + hs);
+          const unsigned ro[3] = {tile_row_off(r0) ^ (16u * cq), tile_row_off(r0 + 1) ^ (16u * cq),
+                                  tile_row_off(r0 + 2) ^ (16u * cq)};
           VecT qd[3], ud;
-          sweep_p1<T>(r, etab, tl, 3 * (EB + hs), cq, vld<T>(vx + cq * W), vld<T>(vy + cq * W), dth, dth3, qd, ud);
+          sweep_p1<T>(r, etab, tl, ro, vld<T>(vx + cq * W), vld<T>(vy + cq * W), vld<T>(vc2 + cq * W), dth, dth3, qd,
+                      ud);
         }
         __syncthreads();
         // the other buffer's tile k - 1 is stored (or being stored): load tile k + 1
@@ -961,43 +897,36 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : (E
         }
 
         // ---- phase 2: the update of block element j, chunks CPT*hh ..
-        // CPT*hh + CPT - 1.  Row offsets are taken at chunk CPT*hh; chunk
-        // CPT*hh + cc of the same row is at offset ^ 16*cc (CPT*hh is a
-        // multiple of CPT, so CPT*hh + cc = CPT*hh ^ cc).
+        // CPT*hh + CPT - 1 (row offsets own[], srcp[], srcq[] are at chunk
+        // CPT*hh; chunk CPT*hh + cc of the same row is at offset ^ 16*cc)
         T rmt = (T)0, sqt = (T)0;
-        unsigned own[3];
-#pragma unroll
-        for (int i = 0; i < 3; ++i) own[i] = tile_off(3 * j + i, CPT * hh);
         VecT outv[CPT][3];
         if (j < nb) {
           const ElemRec<T>& r = recs[j];
-          const int e = e0 + j;
-          const T area3 = r.area * third;
-          T mudt[3], mmdt[3], cmx[3], cmn[3];
+          // per edge: the flux source's rows, AL*n where the edge carries
+          // the element-centric flux (zero on inflow and wall sides, whose
+          // flux the wall path adds); MU*DTE, MM*DTE
+          const int flags = r.flags;
+          unsigned srcp[3], srcq[3];
+          T anx[3], any[3], mudt[3], mmdt[3], cmx[3], cmn[3];
+#pragma unroll
+          for (int k2 = 0; k2 < 3; ++k2) {
+            const ElemEdge<T> ed = r.edge[k2];
+            srcp[k2] = ed.offp ^ hx;
+            srcq[k2] = ed.offq ^ hx;
+            const bool fl = (flags & (FLAG_FLUX0 << k2)) != 0;
+            anx[k2] = fl ? ed.anx : (T)0;
+            any[k2] = fl ? ed.any : (T)0;
+          }
 #pragma unroll
           for (int i = 0; i < 3; ++i) {
             mudt[i] = r.mu[i] * dt;
             mmdt[i] = r.mm[i] * dt;
             if (IMMAT == 0) {
-              cmx[i] = C.cmax[3 * e + i];
-              cmn[i] = C.cmin[3 * e + i];
+              cmx[i] = C.cmax[3 * (e0 + j) + i];
+              cmn[i] = C.cmin[3 * (e0 + j) + i];
             }
           }
-          // per edge: the flux source's rows and AL*n (zero on inflow and
-          // wall sides, whose flux the wall path adds)
-          unsigned srcp[3], srcq[3];
-          T anx[3], any[3];
-#pragma unroll
-          for (int k2 = 0; k2 < 3; ++k2) {
-            const int inf = r.edge[k2].info, kind = inf & 3;
-            const int r0 = 3 * (inf >> 8);
-            srcp[k2] = tile_off(r0 + ((inf >> 3) & 3), CPT * hh);
-            srcq[k2] = tile_off(r0 + ((inf >> 5) & 3), CPT * hh);
-            const T al = (kind == 0 || kind == 2) ? r.edge[k2].alen : (T)0;
-            anx[k2] = al * r.edge[k2].nx;
-            any[k2] = al * r.edge[k2].ny;
-          }
-          const int flags = r.flags;
 #pragma unroll
           for (int cc = 0; cc < CPT; ++cc) {
             const int cq = CPT * hh + cc;
@@ -1013,16 +942,23 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : (E
             VecT g[3];
 #pragma unroll
             for (int i = 0; i < 3; ++i) g[i] = vld<T>(tl + (own[i] ^ cx16));
-            // GETELC second half: RHS_i = AREA*(N_i,x FXME + N_i,y FYME), FXME
-            // = cx * mean(g), FYME = cy * mean(g); the P1 gradients sum to
-            // zero, so RHS_3 = -(RHS_1 + RHS_2)
-            T rhs[3][W];
-#if DGBGK_SWEEP_PACKED32 >= 2
-            if constexpr (sizeof(T) == 4) {
-              sweep_rhs_packed(r, area3, cxv, cyv, g, tl, srcp, srcq, cx16, anx, any, rhs);
-            } else
-#endif
-            {
+            // GETELC second half, the volume term RHS_i = AREA/3 (N_i,x cx +
+            // N_i,y cy) sum(g) (src/getelc.f90:87-117).  For P1,
+            // AREA/3 grad N_i = -(EL/6) n of the edge opposite node i, so an
+            // element whose three sides are interior (AL*n of every edge at
+            // hand) takes RHS_i = -AL*c.n(edge (i+1) mod 3) * sum(g), added
+            // in the edge loop below (sgm = sum(g)); the others use the
+            // gradients, with RHS_3 = -(RHS_1 + RHS_2) from the gradients
+            // summing to zero (sgm = 0)
+            T rhs[3][W], sgm[W];
+            if (flags & FLAG_INTERIOR) {
+#pragma unroll
+              for (int w = 0; w < W; ++w) {
+                sgm[w] = VO::get(g[0], w) + VO::get(g[1], w) + VO::get(g[2], w);
+                rhs[0][w] = rhs[1][w] = rhs[2][w] = (T)0;
+              }
+            } else {
+              const T area3 = r.area * third;
 #pragma unroll
               for (int w = 0; w < W; ++w) {
                 const T cx = VO::get(cxv, w), cy = VO::get(cyv, w);
@@ -1030,21 +966,27 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : (E
                 rhs[0][w] = (r.gx[0] * cx + r.gy[0] * cy) * s3;
                 rhs[1][w] = (r.gx[1] * cx + r.gy[1] * cy) * s3;
                 rhs[2][w] = -(rhs[0][w] + rhs[1][w]);
+                sgm[w] = (T)0;
               }
-              // edge fluxes: RHS_p -= AL*SC*(2 u_p + u_q), RHS_q -= AL*SC*(u_p + 2 u_q)
+            }
+            // edge fluxes (EDGFLXOPT, src/edgflxopt.f90:95-125): RHS_p -=
+            // AL*SC*(2 u_p + u_q), RHS_q -= AL*SC*(u_p + 2 u_q), (u_p, u_q)
+            // the element's own values where AL*SC > 0, the source's
+            // otherwise; AL*SC is zero on sides without the element-centric
+            // flux.  The node opposite the edge takes the volume term.
 #pragma unroll
-              for (int k2 = 0; k2 < 3; ++k2) {
-                const int p = k2, qn = (k2 + 1) % 3;
-                const VecT gp = vld<T>(tl + (srcp[k2] ^ cx16)), gq = vld<T>(tl + (srcq[k2] ^ cx16));
+            for (int k2 = 0; k2 < 3; ++k2) {
+              const int p = k2, qn = (k2 + 1) % 3, op = (k2 + 2) % 3;
+              const VecT gp = vld<T>(tl + (srcp[k2] ^ cx16)), gq = vld<T>(tl + (srcq[k2] ^ cx16));
 #pragma unroll
-                for (int w = 0; w < W; ++w) {
-                  const T as = anx[k2] * VO::get(cxv, w) + any[k2] * VO::get(cyv, w);
-                  const bool mine = as > (T)0;
-                  const T up = mine ? VO::get(g[p], w) : VO::get(gp, w);
-                  const T uq = mine ? VO::get(g[qn], w) : VO::get(gq, w);
-                  rhs[p][w] -= as * ((T)2 * up + uq);
-                  rhs[qn][w] -= as * (up + (T)2 * uq);
-                }
+              for (int w = 0; w < W; ++w) {
+                const T as = anx[k2] * VO::get(cxv, w) + any[k2] * VO::get(cyv, w);
+                const bool mine = as > (T)0;
+                const T up = mine ? VO::get(g[p], w) : VO::get(gp, w);
+                const T uq = mine ? VO::get(g[qn], w) : VO::get(gq, w);
+                rhs[p][w] -= as * ((T)2 * up + uq);
+                rhs[qn][w] -= as * (up + (T)2 * uq);
+                rhs[op][w] -= as * sgm[w];
               }
             }
             // ALPHA < 1: bit 3*w + i marks node i at velocity vb + w as
@@ -1062,15 +1004,15 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : (E
                 const int bs = r.bside[k2];
                 const T twr = (T)2 * C.rgas * C.bTw[bs];
                 const T uwx = C.bUw[2 * bs], uwy = C.bUw[2 * bs + 1], eta = C.bEta[bs];
-                const T nx = r.edge[k2].nx, ny = r.edge[k2].ny, alw = r.edge[k2].alen;
+                const T wnx = r.edge[k2].anx, wny = r.edge[k2].any;  // AL*n of the wall side
                 // with the specular part, the wall branch is taken where the
                 // host's FP64 TEST < 0 (the items of k_wspec are built from it)
                 const int* rfi = spec ? C.rf_i + (size_t)C.rside[bs] * C.V * 2 : nullptr;
 #pragma unroll
                 for (int w = 0; w < W; ++w) {
                   const T cx = VO::get(cxv, w), cy = VO::get(cyv, w);
-                  const T sc = nx * cx + ny * cy;
-                  const bool own = spec ? !(vb + w < C.V && rfi[2 * (vb + w)] >= 0) : sc >= (T)0;
+                  const T asw = wnx * cx + wny * cy;  // AL * (n.c), the sign of TEST
+                  const bool own = spec ? !(vb + w < C.V && rfi[2 * (vb + w)] >= 0) : asw >= (T)0;
                   T up, uq;
                   if (own) {
                     up = VO::get(g[p], w);
@@ -1087,9 +1029,8 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : (E
                     up = uq = C.alpha * (mw * eta);
                     if (spec) dmask |= ((1u << p) | (1u << qn)) << (3 * w);
                   }
-                  const T as = alw * sc;
-                  rhs[p][w] -= as * ((T)2 * up + uq);
-                  rhs[qn][w] -= as * (up + (T)2 * uq);
+                  rhs[p][w] -= asw * ((T)2 * up + uq);
+                  rhs[qn][w] -= asw * (up + (T)2 * uq);
                 }
               }
             }
@@ -1117,18 +1058,22 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : (E
                     rr = ((x >= (T)0) ? cmx[i] : cmn[i]) * x + cdt;
                     rr = rr > (T)0 ? rr : (T)0;
                   }
-                  T fn = f + d;
                   // L2 residual: the change the unknown receives (-f where
-                  // the clip applies; none at inflow-reset nodes)
-                  const T ch = (fn < (T)0) ? -f : d;
-                  fn = fn > (T)0 ? fn : (T)0;
+                  // the clip applies, i.e. where d < -f; none at
+                  // inflow-reset nodes); a non-finite d or f reaches the sum
+                  T ch;
+                  if constexpr (sizeof(T) == 4)
+                    ch = fmax_nan(d, -f);
+                  else
+                    ch = (f + d < (T)0) ? -f : d;
+                  T fn = fmax(f + d, (T)0);
                   if (live) {
                     if (decltype(defer)::value && ((dmask >> (3 * w + i)) & 1u)) {
                       // deferred: k_wspec adds the specular part, clips and
                       // counts the residual
                       C.wd[((size_t)r.wslot * 3 + i) * C.Vp + vb + w] = d;
                     } else {
-                      rmt = rr > rmt ? rr : rmt;
+                      rmt = fmax(rmt, rr);
                       if (!(flags & (1 << i))) sqt += ch * ch;
                     }
                   } else {
@@ -1258,7 +1203,7 @@ template <class T> __global__ void __launch_bounds__(256) k_wspec(const __grid_c
       const int p = k, q = (k + 1) % 3;
       const T dp = om * ((zd2 * F(p, i1) + zd1 * F(p, i2)) / (zd1 + zd2));
       const T dq = om * ((zd2 * F(q, i1) + zd1 * F(q, i2)) / (zd1 + zd2));
-      const T as = r.edge[k].alen * (r.edge[k].nx * cx + r.edge[k].ny * cy);
+      const T as = r.edge[k].anx * cx + r.edge[k].any * cy;  // AL * (n.c)
       drhs[p] -= as * ((T)2 * dp + dq);
       drhs[q] -= as * (dp + (T)2 * dq);
       mask |= (1u << p) | (1u << q);

@@ -20,17 +20,23 @@ namespace dgbgk {
 // The sweep forms every edge flux from an upwind "source" row set: the
 // neighbour across an interior side, the element itself on an outflow side
 // (the upwind value of an outflow side is always the element's own) and, as a
-// placeholder with zero length, on inflow sides (no flux) and wall sides
-// (whose flux the wall path adds).  info bits: [0,2) kind -- 0 interior side,
-// 1 inflow side, 2 outflow side, 3 wall side (any other BSIDO type);
-// [3,5) the source's local node at my point k; [5,7) at my point k+1;
-// [8,32) the source's slot in the sweep tile (block element j: slot j; halo
-// element h: slot EB + h).
+// placeholder, on inflow sides (no flux) and wall sides (whose flux the wall
+// path adds).  The source's two rows (its local nodes at my points k and
+// k+1) are given as their byte offsets in the sweep tile at velocity chunk 0
+// (tile_row_off below); chunk c of the same row is at offset ^ 16*c.
 template <class T> struct alignas(16) ElemEdge {
-  T nx, ny;   // outward unit normal of this element on this edge
-  T alen;     // EL/6 (interior) or RSIDO(3)/6 (boundary)
-  int info;
+  T anx, any;      // AL times the outward unit normal; AL = EL/6 (interior) or RSIDO(3)/6 (boundary)
+  unsigned offp;   // tile offset of the source's row at point k
+  unsigned offq;   // ... at point k+1
 };
+
+// Byte offset of 16-byte chunk 0 of row r in a sweep tile (64-byte rows
+// with the 64-byte swizzle: chunk c of row r at 16*(c ^ ((r >> 1) & 3)),
+// i.e. at tile_row_off(r) ^ 16*c).
+#if defined(__CUDACC__)
+__host__ __device__
+#endif
+inline unsigned tile_row_off(int r) { return (unsigned)(r * 64 + 16 * ((r >> 1) & 3)); }
 
 // Everything the sweep needs about one element, in one 16-byte-aligned
 // record.  The leading part (shape-function gradients and the GTEQNF /
@@ -38,20 +44,32 @@ template <class T> struct alignas(16) ElemEdge {
 // needs; the moment kernel rewrites the node parameters every step.
 template <class T> struct alignas(16) ElemRec {
   T gx[3], gy[3];  // shape-function gradients GEOME(1:3), GEOME(4:6)
-  T A[3];    // DISND*BETA2/PI   (0 where DISPS < 1e-20: NFO = 0, src/gteqnf.f90:32)
-  T ex[3];   // exponent coefficient of NFO: -BETA2 (FP64), -BETA2*log2(e) (FP32, for 2^x)
-  T ux[3];   // DISUX
-  T uy[3];   // DISUY
+  // GTEQNF's Maxwellian NFO (src/gteqnf.f90:26-40) at node i and velocity c,
+  // with A = DISND*BETA2/PI and u = (DISUX, DISUY):
+  //  FP32: NFO = A * 2^(ex*|c-u|^2), ex = -BETA2*log2(e): A, ex, ux, uy;
+  //  FP64: NFO = exp(a0 + a1*cx + a2*cy + ex*|c|^2), the exponent expanded:
+  //        A holds a0 = ln(A) - BETA2*|u|^2, ux a1 = 2*BETA2*ux, uy a2 =
+  //        2*BETA2*uy, ex = -BETA2 (a0 = -inf where A = 0).
+  // (NFO = 0 where DISPS < 1e-20, src/gteqnf.f90:32.)
+  T A[3];
+  T ex[3];
+  T ux[3];
+  T uy[3];
   T mu[3];   // collision frequency MU (src/compmu.f90:90-92)
   T area;    // 0.5 * GEOME(7)   (src/getelc.f90:44)
   T mm[3];   // MMAT (IMMAT = 1) or CMMAT row sums (IMMAT = 0)
   int bside[3];  // boundary side index of each wall edge (kind 3), else -1
   ElemEdge<T> edge[3];
   int flags;  // bits [0,3): DG node i sits on an inflow-side node (INFLOW);
-              // bits [3,6): edge k is a wall side
+              // bits [3,6): edge k is a wall side; bits [6,9): edge k carries
+              // the element-centric flux (interior or outflow side); bit 9:
+              // all three edges are interior sides
   int wslot;  // wall element slot (ALPHA < 1: the deferred updates), else -1
-  int pad1[2];
+  unsigned own01;  // tile offsets (chunk 0) of the element's own rows 0 and 1 (16 bits each)
+  unsigned own2;   // ... and row 2
 };
+constexpr int FLAG_FLUX0 = 1 << 6;      // FLAG_FLUX0 << k: edge k carries the element-centric flux
+constexpr int FLAG_INTERIOR = 1 << 9;  // all three edges interior
 static_assert(sizeof(ElemRec<float>) == 176 && sizeof(ElemRec<double>) == 336, "record layout");
 // values of the leading part a halo element needs (gx .. mu)
 constexpr int REC_HEAD_VALUES = 21;

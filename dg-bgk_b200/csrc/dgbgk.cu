@@ -97,6 +97,7 @@ struct ImplBase {
   int nsm = 148;
   double ref_host = 0.0;
   float last_ms = 0.f;
+  int mom_rows_req = 0;  // moment rows per warp step asked for at create (0: the heuristic)
   // bumped when the case's device table entry changes (buffers moved,
   // re-blocked): a batch holding the case rebuilds its table
   unsigned gen = 0;
@@ -130,7 +131,7 @@ template <class T> struct LaunchSet {
 
 template <class T> using MomFn = void (*)(BatchArgs<T>, int, const CaseDev<T>);
 template <class T, bool ONE> MomFn<T> mom_fn1(int R) {
-  return R == 4 ? k_moments<T, 4, ONE> : R == 2 ? k_moments<T, 2, ONE> : k_moments<T, 1, ONE>;
+  return R == 4 ? k_moments<T, 4, ONE> : R == 3 ? k_moments<T, 3, ONE> : R == 2 ? k_moments<T, 2, ONE> : k_moments<T, 1, ONE>;
 }
 template <class T> MomFn<T> mom_fn(int R, bool one) { return one ? mom_fn1<T, true>(R) : mom_fn1<T, false>(R); }
 template <class T> using SweepFn = void (*)(BatchArgs<T>, int, const CaseDev<T>);
@@ -180,11 +181,11 @@ inline int tiles_per_unit(long total_tiles, int grid0, int upc, int nvt) {
 // Uploads the case table and picks the launch shapes.  Moments: per-warp
 // rings of R-row stages; picks (R, warps per CTA, ring stages) with the most
 // resident warps per SM (shared memory and registers), then the most rows in
-// flight, then the fewest rows per warp step.  Measured on B200 at 24x48
-// velocities: one row per warp step was fastest in FP32 and FP64; warps
-// count for more than stages (FP64: 20 warps with one-stage rings 0.344 ms,
-// 16 with one 0.372, 10 with two 0.486; FP32: 20 with one 0.204, 16 with
-// two 0.207).
+// flight, then the fewest rows per warp step (FP32 takes the element mode
+// first, below).  Measured on B200 at 24x48 velocities, one row per warp
+// step against two or four: warps count for more than stages (FP64: 20 warps
+// with one-stage rings 0.344 ms, 16 with one 0.372, 10 with two 0.486; FP32:
+// 20 with one 0.204, 16 with two 0.207).
 template <class T>
 int build_launch_set(LaunchSet<T>& L, const std::vector<CaseDev<T>>& cs, int eb, int immat, int max_halo, int nsm,
                      cudaStream_t st, int force_rows = 0) {
@@ -199,7 +200,7 @@ int build_launch_set(LaunchSet<T>& L, const std::vector<CaseDev<T>>& cs, int eb,
   const size_t tbytes = one ? (3 * (size_t)cs[0].Vp * sizeof(T) + 127) / 128 * 128 : 0;
   const size_t cap = 227 * 1024;
   long best = -1;
-  for (int R : {4, 2, 1})
+  for (int R : {4, 3, 2, 1})
     for (int w : {20, 16, 12, 10, 8, 6, 5, 4, 3, 2, 1})
       for (int sg : {3, 2, 1}) {
         if (force_rows > 0 && R != force_rows) continue;
@@ -213,7 +214,13 @@ int build_launch_set(LaunchSet<T>& L, const std::vector<CaseDev<T>>& cs, int eb,
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, mfn, w * 32, bytes));
         blocks = std::min(blocks, 4);
         if (blocks < 1) continue;
-        const long score = ((long)blocks * w * 1024 + (long)blocks * w * (sg - 1) * R) * 8 + (8 - R);
+        long score = ((long)blocks * w * 1024 + (long)blocks * w * (sg - 1) * R) * 8 + (8 - R);
+        // FP32: the element mode (R = 3: three rows per warp step sharing
+        // the velocity tables) first, while it keeps 8 or more warps per SM
+        // (measured on the 200x100 channel at 24x48 velocities: 0.158 ms,
+        // against 0.191 with one row per warp step; FP64 loses occupancy
+        // with it: 0.387 against 0.325)
+        if (R == 3 && force_rows == 0) score = (sizeof(T) == 4 && blocks * w >= 8) ? score + (1L << 40) : -1;
         if (score > best) {
           best = score;
           L.mom_rows = R;
@@ -595,7 +602,7 @@ template <class T> struct Impl : ImplBase {
   int refresh() {
     ++gen;
     fill_case();
-    TRY(build_launch_set(single, std::vector<CaseDev<T>>{hc}, pl.EB, pl.immat, pl.max_halo, nsm, st));
+    TRY(build_launch_set(single, std::vector<CaseDev<T>>{hc}, pl.EB, pl.immat, pl.max_halo, nsm, st, mom_rows_req));
     drop_graphs();
     return 0;
   }
@@ -1171,6 +1178,11 @@ int dgbgk_create(const dgbgk_mesh* mesh, const dgbgk_vspace* vs, const dgbgk_par
     impl.reset(new Impl<float>());
   impl->device = prm->device;
   impl->prec = prm->precision;
+  if (prm->moment_rows < 0 || prm->moment_rows > 4) {
+    set_error("dgbgk_create: moment_rows must be 0 (the library's choice) or 1 to 4");
+    return DGBGK_EINVAL;
+  }
+  impl->mom_rows_req = prm->moment_rows;
   std::string err;
   const int eb0 = prm->tile_elems > 0      ? prm->tile_elems
                   : prm->precision == 64 ? Impl<double>::default_eb()
@@ -1338,7 +1350,7 @@ template <class T> struct BatchImpl : BatchBase {
   int* d_done = nullptr;
   int* h_done = nullptr;  // pinned [2]
   int rows = 0;           // moment rows per warp step (0: the heuristic)
-  // ms per step: (eb 64, 128) x (upc 2, 4, 8, 16), then moment rows 1, 2, 4;
+  // ms per step: (eb 64, 128) x (upc 2, 4, 8, 16), then moment rows 1, 2, 3, 4;
   // 0 = not tried
   std::vector<double> tune_ms;
   // per case: the handle's table generation the launch set was built from
@@ -1380,7 +1392,7 @@ template <class T> struct BatchImpl : BatchBase {
     for (auto& e : evp) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     TRY(dalloc(&d_done, 1));
     CK(cudaMallocHost((void**)&h_done, 2 * sizeof(int)));
-    tune_ms.assign(11, 0.0);
+    tune_ms.assign(12, 0.0);
     active.assign(cs.size(), 1);
     stop_rc.assign(cs.size(), 0);
     stop_epoch.assign(cs.size(), 0);
@@ -1476,7 +1488,7 @@ template <class T> struct BatchImpl : BatchBase {
       *per = ms / std::max(steps, 1);
       return restore();
     };
-    const int ebs[2] = {64, 128}, upcs[4] = {2, 4, 8, 16}, rws[3] = {1, 2, 4};
+    const int ebs[2] = {64, 128}, upcs[4] = {2, 4, 8, 16}, rws[4] = {1, 2, 3, 4};
     double best = 1e300;
     int beb = fixed_eb > 0 ? fixed_eb : 128, bupc = fixed_upc > 0 ? fixed_upc : 8;
     for (int ie = 0; ie < 2 && rc == 0; ++ie) {
@@ -1503,7 +1515,7 @@ template <class T> struct BatchImpl : BatchBase {
     // then the moment kernel's rows per warp step for the chosen sweep shape
     int brows = 0;
     best = 1e300;
-    for (int ir = 0; ir < 3 && rc == 0; ++ir) {
+    for (int ir = 0; ir < 4 && rc == 0; ++ir) {
       if (fixed_rows > 0 && rws[ir] != fixed_rows) continue;
       rows = rws[ir];
       rc = configure(beb, bupc);

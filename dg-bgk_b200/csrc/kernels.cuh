@@ -194,14 +194,24 @@ __device__ __forceinline__ int find_case(const int* __restrict__ off, int n, int
 
 // sqrt by a reciprocal-square-root seed and one Newton step for 1/sqrt(x),
 // y <- y (3 - x y^2)/2, in FP64 (relative error ~1e-14 from a ~1e-7 seed).
+__device__ __forceinline__ float rsqrt_sfu(float x) {
+  float r;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
 __device__ __forceinline__ double sqrt_newton(double x) {
   const float xf = (float)x;
   if (!(xf > 0.f)) return 0.0;
-  const double y0 = (double)rsqrtf(xf);
+  const double y0 = (double)rsqrt_sfu(xf);
   const double y1 = y0 * (1.5 - 0.5 * x * y0 * y0);
   return x * y1;
 }
-__device__ __forceinline__ float sqrt_fast(float x) { return x > 0.f ? x * rsqrtf(x) : 0.f; }
+// FP32 sqrt from the SFU (sqrt.approx: relative error ~2^-23; sqrt(0) = 0)
+__device__ __forceinline__ float sqrt_fast(float x) {
+  float r;
+  asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
 
 // Pass sums over one velocity row in shared memory by the L lanes of a
 // group (lane sub takes 16-byte vectors sub, sub+L, ...).  FP64 storage:
@@ -283,6 +293,111 @@ template <> struct RowMath<float> {
   }
 };
 
+// Pass sums over the three velocity rows of one element by all 32 lanes of
+// a warp (lane l takes 16-byte vectors l, l+32, ...): the velocity tables
+// are loaded once per vector for the three rows.  FP32 storage: FP32 lane
+// partials, summed in FP64 across the warp; FP64 storage: FP64 throughout.
+template <class T> struct ElemMath;
+
+template <> struct ElemMath<float> {
+  static __device__ __forceinline__ void pass1(const float* rows, unsigned pitch, const float* tb, int Vp, int nq,
+                                               int lane, double (&s)[3][3]) {
+    const float4* cx = reinterpret_cast<const float4*>(tb);
+    const float4* cy = reinterpret_cast<const float4*>(tb + Vp);
+    const float4* wj = reinterpret_cast<const float4*>(tb + 2 * Vp);
+    float t[3][3] = {};
+    for (int q = lane; q < nq; q += 32) {
+      const float4 c = cx[q], d = cy[q], w = wj[q];
+#pragma unroll
+      for (int r = 0; r < 3; ++r) {
+        const float4 x = reinterpret_cast<const float4*>(reinterpret_cast<const unsigned char*>(rows) + r * pitch)[q];
+        const float a0 = w.x * x.x, a1 = w.y * x.y, a2 = w.z * x.z, a3 = w.w * x.w;
+        t[r][0] += (a0 + a1) + (a2 + a3);
+        t[r][1] = fmaf(c.x, a0, fmaf(c.y, a1, fmaf(c.z, a2, fmaf(c.w, a3, t[r][1]))));
+        t[r][2] = fmaf(d.x, a0, fmaf(d.y, a1, fmaf(d.z, a2, fmaf(d.w, a3, t[r][2]))));
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int k = 0; k < 3; ++k) s[r][k] = (double)t[r][k];
+  }
+  static __device__ __forceinline__ void pass2(const float* rows, unsigned pitch, const float* tb, int Vp, int nq,
+                                               int lane, const double (&u)[3][2], double (&s)[3][2]) {
+    const float4* cx = reinterpret_cast<const float4*>(tb);
+    const float4* cy = reinterpret_cast<const float4*>(tb + Vp);
+    const float4* wj = reinterpret_cast<const float4*>(tb + 2 * Vp);
+    float fu[3][2], t[3][2] = {};
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      fu[r][0] = (float)u[r][0];
+      fu[r][1] = (float)u[r][1];
+    }
+    for (int q = lane; q < nq; q += 32) {
+      const float4 c = cx[q], d = cy[q], w = wj[q];
+#pragma unroll
+      for (int r = 0; r < 3; ++r) {
+        const float4 x = reinterpret_cast<const float4*>(reinterpret_cast<const unsigned char*>(rows) + r * pitch)[q];
+        const float e0 = c.x - fu[r][0], e1 = c.y - fu[r][0], e2 = c.z - fu[r][0], e3 = c.w - fu[r][0];
+        const float g0 = d.x - fu[r][1], g1 = d.y - fu[r][1], g2 = d.z - fu[r][1], g3 = d.w - fu[r][1];
+        const float q0 = fmaf(e0, e0, g0 * g0), q1 = fmaf(e1, e1, g1 * g1), q2 = fmaf(e2, e2, g2 * g2),
+                    q3 = fmaf(e3, e3, g3 * g3);
+        const float a0 = w.x * x.x, a1 = w.y * x.y, a2 = w.z * x.z, a3 = w.w * x.w;
+        t[r][0] = fmaf(q0, a0, fmaf(q1, a1, fmaf(q2, a2, fmaf(q3, a3, t[r][0]))));  // src/macros.f90:144-148
+        t[r][1] = fmaf(sqrt_fast(q0), a0,
+                       fmaf(sqrt_fast(q1), a1, fmaf(sqrt_fast(q2), a2, fmaf(sqrt_fast(q3), a3, t[r][1]))));
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      s[r][0] = 0.5 * (double)t[r][0];
+      s[r][1] = (double)t[r][1];
+    }
+  }
+};
+
+template <> struct ElemMath<double> {
+  static __device__ __forceinline__ void pass1(const double* rows, unsigned pitch, const double* tb, int Vp, int nq,
+                                               int lane, double (&s)[3][3]) {
+    const double2* cx = reinterpret_cast<const double2*>(tb);
+    const double2* cy = reinterpret_cast<const double2*>(tb + Vp);
+    const double2* wj = reinterpret_cast<const double2*>(tb + 2 * Vp);
+#pragma unroll
+    for (int r = 0; r < 3; ++r) s[r][0] = s[r][1] = s[r][2] = 0.0;
+    for (int q = lane; q < nq; q += 32) {
+      const double2 c = cx[q], d = cy[q], w = wj[q];
+#pragma unroll
+      for (int r = 0; r < 3; ++r) {
+        const double2 x = reinterpret_cast<const double2*>(reinterpret_cast<const unsigned char*>(rows) + r * pitch)[q];
+        const double a0 = w.x * x.x, a1 = w.y * x.y;
+        s[r][0] += a0 + a1;
+        s[r][1] = fma(c.x, a0, fma(c.y, a1, s[r][1]));
+        s[r][2] = fma(d.x, a0, fma(d.y, a1, s[r][2]));
+      }
+    }
+  }
+  static __device__ __forceinline__ void pass2(const double* rows, unsigned pitch, const double* tb, int Vp, int nq,
+                                               int lane, const double (&u)[3][2], double (&s)[3][2]) {
+    const double2* cx = reinterpret_cast<const double2*>(tb);
+    const double2* cy = reinterpret_cast<const double2*>(tb + Vp);
+    const double2* wj = reinterpret_cast<const double2*>(tb + 2 * Vp);
+#pragma unroll
+    for (int r = 0; r < 3; ++r) s[r][0] = s[r][1] = 0.0;
+    for (int q = lane; q < nq; q += 32) {
+      const double2 c = cx[q], d = cy[q], w = wj[q];
+#pragma unroll
+      for (int r = 0; r < 3; ++r) {
+        const double2 x = reinterpret_cast<const double2*>(reinterpret_cast<const unsigned char*>(rows) + r * pitch)[q];
+        const double dx0 = c.x - u[r][0], dy0 = d.x - u[r][1], dx1 = c.y - u[r][0], dy1 = d.y - u[r][1];
+        const double q0 = dx0 * dx0 + dy0 * dy0, q1 = dx1 * dx1 + dy1 * dy1;
+        const double a0 = w.x * x.x, a1 = w.y * x.y;
+        s[r][0] = fma(0.5 * q0, a0, fma(0.5 * q1, a1, s[r][0]));                // src/macros.f90:144-148
+        s[r][1] = fma(sqrt_newton(q0), a0, fma(sqrt_newton(q1), a1, s[r][1]));  // src/compmu.f90:71-74
+      }
+    }
+  }
+};
+
 // Sum over the L lanes of an aligned lane group (every lane gets the same
 // bits: each butterfly level adds the same two operands in either order).
 template <int L> __device__ __forceinline__ double group_sum(double v) {
@@ -303,10 +418,14 @@ template <int L> __device__ __forceinline__ double group_sum(double v) {
 template <class T, int R, bool ONE>
 __global__ void __launch_bounds__(ONE ? 640 : 512, 1)
     k_moments(BatchArgs<T> a, int total_groups, const __grid_constant__ CaseDev<T> one) {
-  constexpr int L = 32 / R;
+  // R = 1, 2, 4: R rows of any elements per warp step, 32/R lanes per row;
+  // R = 3: the three rows of one element per warp step, all 32 lanes on
+  // each (the velocity tables loaded once for the three rows)
+  constexpr bool ELEM = R == 3;
+  constexpr int L = ELEM ? 32 : 32 / R;
   extern __shared__ __align__(128) unsigned char sm_raw[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-  const int grp = lane / L, sub = lane % L;
+  const int grp = ELEM ? 0 : lane / L, sub = lane % L;
   const int nstage = a.mom_stages;
   // layout: [barriers][tables [3][Vp] (ONE)][rings: warp, stage, R rows]
   uint64_t* bars = reinterpret_cast<uint64_t*>(sm_raw) + warp * nstage;
@@ -368,26 +487,65 @@ __global__ void __launch_bounds__(ONE ? 640 : 512, 1)
       flush_mu();
       mu_case = c;
     }
-    const int node = (g - (ONE ? 0 : a.grp_off[c])) * R + grp;
+    const int node0 = (g - (ONE ? 0 : a.grp_off[c])) * R;
     const T* tb = ONE ? tb1 : C.tabs;
-    const bool live = !C.ctrl->done && node < 3 * C.E;
-    const T* row = reinterpret_cast<const T*>(ring + (size_t)s * stage_bytes + (size_t)grp * C.rowbytes);
-    const int nql = live ? (int)(C.rowbytes / 16) : 0;
-    double s0 = 0, s1 = 0, s2 = 0;
-    RowMath<T>::pass1(row, tb, C.Vp, nql, sub, L, s0, s1, s2);
-    s0 = group_sum<L>(s0);
-    s1 = group_sum<L>(s1);
-    s2 = group_sum<L>(s2);
-    double nd = 0, ux = 0, uy = 0;
-    if (s0 >= TINY_D) {  // src/macros.f90:126-134
-      nd = s0;
-      ux = s1 / s0;
-      uy = s2 / s0;
+    const bool live0 = !C.ctrl->done;
+    const int nql = live0 ? (int)(C.rowbytes / 16) : 0;
+    // this lane's node and its sums: s0 = n, ux, uy (MACROS pass 1), sp, sc
+    // (pass 2: pressure and COMPMU's mean relative speed)
+    int node;
+    double s0, ux, uy, nd, sp, sc;
+    if constexpr (ELEM) {
+      const T* rows = reinterpret_cast<const T*>(ring + (size_t)s * stage_bytes);
+      double m1[3][3], u[3][2], m2[3][2];
+      ElemMath<T>::pass1(rows, C.rowbytes, tb, C.Vp, nql, lane, m1);
+#pragma unroll
+      for (int r = 0; r < 3; ++r) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) m1[r][k] = group_sum<32>(m1[r][k]);
+        u[r][0] = u[r][1] = 0.0;
+        if (m1[r][0] >= TINY_D) {  // src/macros.f90:126-134
+          u[r][0] = m1[r][1] / m1[r][0];
+          u[r][1] = m1[r][2] / m1[r][0];
+        }
+      }
+      ElemMath<T>::pass2(rows, C.rowbytes, tb, C.Vp, nql, lane, u, m2);
+#pragma unroll
+      for (int r = 0; r < 3; ++r) {
+        m2[r][0] = group_sum<32>(m2[r][0]);
+        m2[r][1] = group_sum<32>(m2[r][1]);
+      }
+      // lanes 0, 1, 2 write rows 0, 1, 2
+      const int r = lane < 3 ? lane : 0;
+      node = node0 + r;
+      s0 = r == 0 ? m1[0][0] : r == 1 ? m1[1][0] : m1[2][0];
+      ux = r == 0 ? u[0][0] : r == 1 ? u[1][0] : u[2][0];
+      uy = r == 0 ? u[0][1] : r == 1 ? u[1][1] : u[2][1];
+      sp = r == 0 ? m2[0][0] : r == 1 ? m2[1][0] : m2[2][0];
+      sc = r == 0 ? m2[0][1] : r == 1 ? m2[1][1] : m2[2][1];
+      nd = s0 >= TINY_D ? s0 : 0.0;
+    } else {
+      node = node0 + grp;
+      const T* row = reinterpret_cast<const T*>(ring + (size_t)s * stage_bytes + (size_t)grp * C.rowbytes);
+      const int nqr = node < 3 * C.E ? nql : 0;
+      double s1 = 0, s2 = 0;
+      s0 = 0;
+      RowMath<T>::pass1(row, tb, C.Vp, nqr, sub, L, s0, s1, s2);
+      s0 = group_sum<L>(s0);
+      s1 = group_sum<L>(s1);
+      s2 = group_sum<L>(s2);
+      nd = ux = uy = 0;
+      if (s0 >= TINY_D) {  // src/macros.f90:126-134
+        nd = s0;
+        ux = s1 / s0;
+        uy = s2 / s0;
+      }
+      sp = sc = 0;
+      RowMath<T>::pass2(row, tb, C.Vp, nqr, sub, L, ux, uy, sp, sc);
+      sp = group_sum<L>(sp);
+      sc = group_sum<L>(sc);
     }
-    double sp = 0, sc = 0;
-    RowMath<T>::pass2(row, tb, C.Vp, nql, sub, L, ux, uy, sp, sc);
-    sp = group_sum<L>(sp);
-    sc = group_sum<L>(sc);
+    const bool live = live0 && node < 3 * C.E;
     __syncwarp();
     // the rows are consumed: refill this stage with the group nstage ahead
     if (lane == 0) {
@@ -397,7 +555,7 @@ __global__ void __launch_bounds__(ONE ? 640 : 512, 1)
         fill(s, nxt);
       }
     }
-    if (sub == 0 && live) {
+    if ((ELEM ? lane < 3 : sub == 0) && live) {
       const double ps = sp * C.MM;
       const double ct = (nd >= TINY_D) ? sc / nd : 0.0;
       const double mu = sqrt(2.0) * ct * C.sigt * nd;
@@ -911,12 +1069,11 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : (E
           T anx[3], any[3], mudt[3], mmdt[3], cmx[3], cmn[3];
 #pragma unroll
           for (int k2 = 0; k2 < 3; ++k2) {
-            const ElemEdge<T> ed = r.edge[k2];
-            srcp[k2] = ed.offp ^ hx;
-            srcq[k2] = ed.offq ^ hx;
+            srcp[k2] = r.edge[k2].offp ^ hx;
+            srcq[k2] = r.edge[k2].offq ^ hx;
             const bool fl = (flags & (FLAG_FLUX0 << k2)) != 0;
-            anx[k2] = fl ? ed.anx : (T)0;
-            any[k2] = fl ? ed.any : (T)0;
+            anx[k2] = fl ? r.edge[k2].anx : (T)0;
+            any[k2] = fl ? r.edge[k2].any : (T)0;
           }
 #pragma unroll
           for (int i = 0; i < 3; ++i) {

@@ -30,7 +30,7 @@ extern "C" void dgbgk_default_params(dgbgk_params* p) {
   p->precision = 64;
   p->wall_velocity = nullptr;
   p->tile_elems = 0;
-  p->tile_vels = 0;
+  p->moment_rows = 0;
   p->device = 0;
 }
 

@@ -47,7 +47,7 @@ class Params(ctypes.Structure):
         ("immat", c_int), ("csafm", c_double), ("alpha", c_double), ("rgas", c_double),
         ("molar_mass", c_double), ("diameter", c_double), ("cinf", c_double * 4),
         ("precision", c_int), ("wall_velocity", POINTER(c_double)),
-        ("tile_elems", c_int), ("tile_vels", c_int), ("device", c_int),
+        ("tile_elems", c_int), ("moment_rows", c_int), ("device", c_int),
     ]
 
 

@@ -23,6 +23,7 @@ def main(argv=None):
     ap.add_argument("--precision", type=int, default=32, choices=[32, 64])
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--tile-elems", type=int, default=0)
+    ap.add_argument("--moment-rows", type=int, default=0, help="moment rows per warp step (1-4; 0: the library's)")
     ap.add_argument("--lib", default=None, help="a library build to time instead of lib/libdgbgk.so "
                     "(e.g. a compile-time variant from `make variant`)")
     a = ap.parse_args(argv)
@@ -30,7 +31,7 @@ def main(argv=None):
         from . import _lib
         _lib.use_library(a.lib)
     case = CONFIGS[a.config]()
-    s = Solver.from_case(case, precision=a.precision, tile_elems=a.tile_elems)
+    s = Solver.from_case(case, precision=a.precision, tile_elems=a.tile_elems, moment_rows=a.moment_rows)
     s.init_case()
     s.advance(2)
     ms = s.profile(a.steps)

@@ -69,7 +69,7 @@ class Solver:
 
     def __init__(self, intma, coord, bsido, setup, vcord, sumweight, rorder, torder, rv, *, immat=1, csafm=0.5,
                  alpha=1.0, rgas=1.0, molar_mass=6.022e26, diameter=1.0, cinf=(0, 0, 0, 0), precision=64,
-                 wall_velocity=None, tile_elems=0, device=0):
+                 wall_velocity=None, tile_elems=0, moment_rows=0, device=0):
         L = lib()
         self._keep = []
 
@@ -111,6 +111,7 @@ class Solver:
         p.precision = precision
         p.wall_velocity = ptr(keep(wall_velocity)) if wall_velocity is not None else None
         p.tile_elems = tile_elems
+        p.moment_rows = moment_rows
         p.device = device
         h = c_void_p()
         check(L.dgbgk_create(ctypes.byref(m), ctypes.byref(vs), ctypes.byref(p), ctypes.byref(h)))
@@ -118,7 +119,7 @@ class Solver:
         self.precision = precision
 
     @classmethod
-    def from_case(cls, case, precision=64, tile_elems=0, device=0):
+    def from_case(cls, case, precision=64, tile_elems=0, moment_rows=0, device=0):
         from .cases import gll
         m = case.mesh
         st = setup_mesh(m.intma, m.coord, m.bsido)
@@ -127,7 +128,7 @@ class Solver:
         s = cls(m.intma, m.coord, m.bsido, st, vc, sw, case.rorder, case.torder, case.rv, immat=case.immat,
                 csafm=case.csafm, alpha=case.alpha, rgas=case.rgas, molar_mass=case.molar_mass,
                 diameter=case.diameter, cinf=case.cinf, precision=precision, wall_velocity=m.wall_velocity,
-                tile_elems=tile_elems, device=device)
+                tile_elems=tile_elems, moment_rows=moment_rows, device=device)
         s.case = case
         s.setup = st
         s.vcord = vc
@@ -260,7 +261,7 @@ class Batch:
     must share precision, IMMAT and device; they stay usable on their own
     between batch calls."""
 
-    TUNE_KEYS = [(eb, upc) for eb in (64, 128) for upc in (2, 4, 8, 16)] + [("rows", r) for r in (1, 2, 4)]
+    TUNE_KEYS = [(eb, upc) for eb in (64, 128) for upc in (2, 4, 8, 16)] + [("rows", r) for r in (1, 2, 3, 4)]
 
     def __init__(self, solvers, tile_elems=0, units_per_cta=0, tune_steps=4, moment_rows=0):
         from ._lib import BatchParams
@@ -312,8 +313,8 @@ class Batch:
                          "moment_rows"], (int(x) for x in o)))
 
     def tuning(self):
-        ms = np.zeros(11)
-        check(lib().dgbgk_batch_tuning(self.h, 11, ptr(ms)))
+        ms = np.zeros(12)
+        check(lib().dgbgk_batch_tuning(self.h, 12, ptr(ms)))
         return {k: float(v) for k, v in zip(self.TUNE_KEYS, ms) if v > 0}
 
     def last_ms(self):

@@ -83,7 +83,10 @@ typedef struct dgbgk_params {
   const double* wall_velocity; /* (2,NBOUN) moving-wall velocity per
                                   boundary side, or NULL (all at rest)    */
   int tile_elems;     /* sweep tile: elements per CTA, 64 or 128 (0: 128 for FP32, 64 for FP64) */
-  int tile_vels;      /* sweep tile: velocities per CTA (0 = default)      */
+  int moment_rows;    /* moment kernel: velocity rows per warp step -- 1, 2 or 4
+                         rows of any elements (32/R lanes per row), or 3: the
+                         three rows of one element on all 32 lanes (0 = the
+                         library's choice) */
   int device;         /* CUDA device ordinal                               */
 } dgbgk_params;
 
@@ -229,7 +232,7 @@ typedef struct {
   int tile_elems;     /* sweep elements per CTA, 64 or 128 (0: autotuned)    */
   int units_per_cta;  /* sweep work units per resident CTA, 2/4/8/16 (0: autotuned) */
   int tune_steps;     /* steps timed per autotuner candidate                */
-  int moment_rows;    /* moment rows per warp step, 1/2/4 (0: autotuned)     */
+  int moment_rows;    /* moment rows per warp step, 1/2/3/4 (0: autotuned)   */
 } dgbgk_batch_params;
 
 void dgbgk_batch_default_params(dgbgk_batch_params* p);
@@ -268,8 +271,8 @@ int dgbgk_batch_status(const dgbgk_batch* b, int* status);
 int dgbgk_batch_info(const dgbgk_batch* b, int* out7);
 
 /* The autotuner's ms per batch step: (tile_elems 64, 128) x (units_per_cta
- * 2, 4, 8, 16), then moment rows per warp step 1, 2, 4 at the chosen sweep
- * shape; 0 where not tried; n <= 11. */
+ * 2, 4, 8, 16), then moment rows per warp step 1, 2, 3, 4 at the chosen
+ * sweep shape; 0 where not tried; n <= 12. */
 int dgbgk_batch_tuning(const dgbgk_batch* b, int n, double* ms_per_step);
 
 /* Device time of the last dgbgk_batch_advance() in ms. */

@@ -122,7 +122,7 @@ def stopping_cases():
     ]
 
 
-SHAPES = [(eb, upc, rows) for eb in (64, 128) for upc in (2, 4, 8, 16) for rows in (1, 2, 4)]
+SHAPES = [(eb, upc, rows) for eb in (64, 128) for upc in (2, 4, 8, 16) for rows in (1, 2, 3, 4)]
 
 
 def test_every_batch_shape_with_a_case_stopping_early():

@@ -19,7 +19,7 @@ pytestmark = pytest.mark.gpu
 TOL64 = 1e-10
 
 
-def pair(case, prec=64, oracle_prec=64, tile_elems=0, lobatto=None):
+def pair(case, prec=64, oracle_prec=64, tile_elems=0, lobatto=None, moment_rows=0):
     if lobatto is not None:
         from dgbgk.solver import setup_mesh, vspace
         eta, w = lobatto
@@ -35,7 +35,7 @@ def pair(case, prec=64, oracle_prec=64, tile_elems=0, lobatto=None):
                    alpha=case.alpha, rgas=case.rgas, molar_mass=case.molar_mass, diameter=case.diameter,
                    cinf=case.cinf, immat=case.immat, prec=oracle_prec, wall_velocity=m.wall_velocity)
     else:
-        s = Solver.from_case(case, precision=prec, tile_elems=tile_elems)
+        s = Solver.from_case(case, precision=prec, tile_elems=tile_elems, moment_rows=moment_rows)
         o = Oracle.from_case(case, prec=oracle_prec)
     # identical initial state: the oracle's INICON2 times the per-node scale
     i = case.init
@@ -117,6 +117,26 @@ def test_fp64_steps_match_oracle(mk, steps):
 @pytest.mark.parametrize("prec", [64, 32])
 def test_tile_shapes_agree(tile, prec):
     s, o, f0 = pair(small_channel(), prec=prec, tile_elems=tile)
+    s.advance(3)
+    o.advance(3)
+    assert rel_l2(s.get_state(), o.get_state()) <= (TOL64 if prec == 64 else 1e-5)
+
+
+@pytest.mark.parametrize("rows", [1, 2, 3, 4])
+@pytest.mark.parametrize("prec", [64, 32])
+def test_moment_modes_agree(rows, prec):
+    # every moment-kernel mode (1, 2 or 4 rows of any elements per warp
+    # step, or the three rows of one element) on a ragged velocity count:
+    # the moments, MU and three steps match the oracle
+    c = channel_case(-2.0, 4.0, -2.0, 2.0, 30, 20, 6, 11, mach=2.0, kn=0.05, obstacle_side=1.0)
+    s, o, f0 = pair(c, prec=prec, moment_rows=rows)
+    tol = 1e-13 if prec == 64 else 1e-6
+    ref = o.compmu()
+    got = s.node_fields()
+    assert rel_l2(got["disnd"].ravel(), ref["DISND"]) <= tol
+    assert rel_l2(got["disux"].ravel(), ref["DISUX"], vscale(s)) <= tol
+    assert rel_l2(got["disps"].ravel(), ref["DISPS"]) <= tol
+    assert rel_l2(got["mu"].ravel(), ref["MU"]) <= tol
     s.advance(3)
     o.advance(3)
     assert rel_l2(s.get_state(), o.get_state()) <= (TOL64 if prec == 64 else 1e-5)

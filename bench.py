@@ -53,6 +53,7 @@ def args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-steady", action="store_true", help="skip the time-to-steady-state leg")
     ap.add_argument("--no-tc1", action="store_true", help="skip the reference test case tc1 leg")
+    ap.add_argument("--no-large", action="store_true", help="skip the large-channel (400x200, 32x64) leg")
     return ap.parse_args()
 
 
@@ -65,6 +66,14 @@ def workload(case, prec):
     m = case.mesh
     return (f"{case.name}: {m.nelem} P1 elements x {case.rorder}x{case.torder} velocities = {case.dofs} DOFs, "
             f"Mach {case.info.get('mach')}, Kn {case.info.get('kn')}, f in FP{prec}")
+
+
+def config_of(case, prec, world):
+    """The workload description both arms print (the same keys and values)."""
+    sf = 4 if prec == 32 else 8
+    return {"workload": workload(case, prec), "nelem": case.mesh.nelem, "vnpnt": case.rorder * case.torder,
+            "dofs": case.dofs, "l2": f"inputs larger than L2: each f buffer is {case.dofs * sf / 1e6:.0f} MB",
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
 
 
 # ------------------------------------------------------------------ dist ----
@@ -257,6 +266,33 @@ def tc1_leg(device, steps=40, warmup=3):
     return out
 
 
+def large_leg(device, steps=10, warmup=3):
+    """The large channel ([-10,30]x[-10,10], 400x200 quads, 32x64
+    velocities, 9.8e8 DOFs, Mach 1.5, Kn 0.02): ms per step and the kernels'
+    achieved bandwidth at FP32 and FP64 (the time to steady state of this
+    workload is recorded by dgbgk.steady, not here)."""
+    from dgbgk import Solver, config5
+    case = config5()
+    names = ["k_moments", "k_wall", "k_sweep", "k_resid"]
+    peak, _ = peaks()
+    out = {"workload": workload(case, 32).replace(", f in FP32", ""), "dofs": case.dofs}
+    for prec in (32, 64):
+        sf = 4 if prec == 32 else 8
+        s = Solver.from_case(case, precision=prec, device=device)
+        s.init_case()
+        s.advance(warmup)
+        s.advance(steps)
+        ms = s.last_ms() / steps
+        k = s.profile(3)
+        out[f"fp{prec}"] = {"ms_per_step": ms, "dof_updates_per_s": case.dofs / (ms * 1e-3),
+                            "sweep_gbs": 2 * sf * case.dofs / (k[2] * 1e-3) / 1e9,
+                            "sweep_frac": 2 * sf * case.dofs / (k[2] * 1e-3) / 1e9 / peak,
+                            "moments_gbs": sf * case.dofs / (k[0] * 1e-3) / 1e9,
+                            "kernel_ms": dict(zip(names, [float(x) for x in k]))}
+        s.close()
+    return out
+
+
 # ------------------------------------------------------------- our arm ----
 def run_ours(a, d):
     import numpy as np
@@ -295,11 +331,8 @@ def run_ours(a, d):
            "warmup": a.warmup, "ms_per_step": t_ms / a.steps, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f32" if a.precision == 32 else "f64",
            "data": "synthetic (generated mesh and velocity grid; free-stream initial state)",
-           "config": {"workload": workload(case, a.precision), "nelem": case.mesh.nelem,
-                      "vnpnt": case.rorder * case.torder, "dofs": case.dofs,
-                      "tile_elems": info["tile_elems"], "max_halo": info["max_halo"],
-                      "l2": f"inputs larger than L2: each f buffer is {case.dofs * sf / 1e6:.0f} MB",
-                      "parallelism": f"replicas x{d.world}" if d.world > 1 else "single GPU"},
+           "config": config_of(case, a.precision, d.world),
+           "launch": {"tile_elems": info["tile_elems"], "max_halo": info["max_halo"]},
            "roofline": {"bound": "hbm", "kernel": "k_sweep", "achieved": achieved, "peak": peak, "unit": "GB/s",
                         "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
                         "alg_bytes_per_launch": alg_bytes,
@@ -344,6 +377,8 @@ def run_ours(a, d):
         out["steady_state"] = st
     if not a.no_tc1 and d.world == 1:
         out["reference_case_tc1"] = tc1_leg(d.local)
+    if not a.no_large and d.world == 1:
+        out["large_channel"] = large_leg(d.local)
     # end to end through the C ABI with host buffers
     if not a.no_e2e:
         s = Solver.from_case(case, precision=a.precision, device=d.local)
@@ -351,13 +386,13 @@ def run_ours(a, d):
         host = torch.empty((case.mesh.nelem, case.rorder * case.torder, 3),
                            dtype=torch.float32 if a.precision == 32 else torch.float64).pin_memory()
         hv = host.numpy()
-        hv[...] = s.get_state(hv.dtype.type)
+        s.get_state(out=hv)
         s.advance(2)
         d.barrier()
         t0 = time.perf_counter()
-        s.set_state(hv)                  # H2D of DISNF(3,V,E) + layout change
+        s.set_state(hv)         # H2D of DISNF(3,V,E) from the pinned buffer + layout change
         s.advance(a.steps)
-        hv[...] = s.get_state(hv.dtype.type)  # D2H of the advanced DISNF
+        s.get_state(out=hv)     # layout change + D2H of the advanced DISNF into the pinned buffer
         t1 = time.perf_counter()
         te = d.max(t1 - t0)
         nb = host.numel() * host.element_size()
@@ -384,7 +419,7 @@ def run_reference(a, d):
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": secs * 1e3 / a.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (generated mesh and velocity grid; free-stream initial state)",
-            "config": {"workload": workload(case, 32), "dofs": case.dofs},
+            "config": config_of(case, 32, d.world),
             "cpu_baseline": {"value": rate, "unit": UNIT, "cores": thr, "kind": "port",
                              "sample": f"{a.steps} full pseudo-time steps of {case.name} after {a.warmup} warm-up "
                                        f"steps (FP32, {thr} OpenMP threads)"},

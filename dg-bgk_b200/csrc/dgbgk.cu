@@ -91,6 +91,11 @@ struct ImplBase {
   virtual int snapshot(int slot) = 0;
   virtual int extrapolate(int n, double* gamma) = 0;
   virtual int import_device(const double* buf) = 0;
+  // device observables (GETFOR, and GETMAC every `every` steps into a ring)
+  virtual int forces(double* lift, double* drag) = 0;
+  virtual int set_output(int every, int cap) = 0;
+  virtual int output_count(int* n) = 0;
+  virtual int get_output(int k, int* itime, double* const* fields, double* lift, double* drag) = 0;
   Plan pl;
   int device = 0;
   int prec = 64;
@@ -98,6 +103,7 @@ struct ImplBase {
   double ref_host = 0.0;
   float last_ms = 0.f;
   int mom_rows_req = 0;  // moment rows per warp step asked for at create (0: the heuristic)
+  long long itime_total = 0;  // steps run since the state was last set (the reference's ITIME)
   // bumped when the case's device table entry changes (buffers moved,
   // re-blocked): a batch holding the case rebuilds its table
   unsigned gen = 0;
@@ -298,7 +304,8 @@ inline int launch_check(const char* what, int grid, int block, size_t smem) {
 
 // One pseudo-time step of every case of the set: moments, wall flux, sweep,
 // residual bookkeeping.
-template <class T> int enqueue_step(const LaunchSet<T>& L, cudaStream_t st, float* ms = nullptr) {
+template <class T>
+int enqueue_step(const LaunchSet<T>& L, cudaStream_t st, float* ms = nullptr, const OutArgs* out = nullptr) {
   cudaEvent_t ev[5];
   if (ms)
     for (auto& e : ev) CK(cudaEventCreate(&e));
@@ -306,6 +313,13 @@ template <class T> int enqueue_step(const LaunchSet<T>& L, cudaStream_t st, floa
   mom_fn<T>(L.mom_rows, L.one)<<<L.mom_grid, L.mom_warps * 32, L.mom_smem, st>>>(L.args, L.total_groups,
                                                                                  L.one_case);
   TRY(launch_check("k_moments", L.mom_grid, L.mom_warps * 32, L.mom_smem));
+  if (out) {  // the previous step's GETMAC / GETFOR record, when due
+    const int g = (out->nod.NP + 255) / 256;
+    k_out_nodal<<<g, 256, 0, st>>>(*out);
+    TRY(launch_check("k_out_nodal", g, 256, 0));
+    k_out_forces<<<1, FORCE_THREADS, 0, st>>>(*out);
+    TRY(launch_check("k_out_forces", 1, FORCE_THREADS, 0));
+  }
   if (ms) cudaEventRecord(ev[1], st);
   if (L.total_walls > 0) {
     k_wall<T><<<L.total_walls, WALL_THREADS, 0, st>>>(L.args, L.total_walls);
@@ -381,6 +395,12 @@ template <class T> struct Impl : ImplBase {
   double *d_gram = nullptr, *d_gamma = nullptr;
   CaseDev<T> hc;          // this case's table entry
   LaunchSet<T> single;    // this case alone
+  // device observables: GETFOR's sides, the output ring and one direct record
+  ForceSide* d_fs = nullptr;
+  int out_every = 0, out_cap = 0;
+  double* out_ring = nullptr;
+  int* out_count = nullptr;
+  double* out_direct = nullptr;
 
   ~Impl() override {
     cudaSetDevice(device);
@@ -430,6 +450,10 @@ template <class T> struct Impl : ImplBase {
     dfree(snaps);
     dfree(d_gram);
     dfree(d_gamma);
+    dfree(d_fs);
+    dfree(out_ring);
+    dfree(out_count);
+    dfree(out_direct);
     if (staging) cudaFree(staging);
     if (hctrl) cudaFreeHost(hctrl);
     if (ev0) cudaEventDestroy(ev0);
@@ -497,6 +521,7 @@ template <class T> struct Impl : ImplBase {
     TRY(upload(&node_off, pl.node_off, st));
     TRY(upload(&node_dg, pl.node_dg, st));
     TRY(upload(&node_ae, pl.node_ae, st));
+    TRY(upload(&d_fs, pl.fsides, st));
     if (pl.spec) {
       std::vector<T> rz(pl.rf_z.begin(), pl.rf_z.end());
       TRY(upload(&rside, pl.rside, st));
@@ -699,7 +724,8 @@ template <class T> struct Impl : ImplBase {
     cudaGraph_t g;
     CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     int rc = 0;
-    for (int k = 0; k < GRAPH_STEPS && rc == 0; ++k) rc = enqueue_step(single, st);
+    const OutArgs oa = out_args(-1, nullptr);
+    for (int k = 0; k < GRAPH_STEPS && rc == 0; ++k) rc = enqueue_step(single, st, nullptr, out_every > 0 ? &oa : nullptr);
     cudaError_t e = cudaStreamEndCapture(st, &g);
     if (rc != 0) return rc;
     CK(e);
@@ -715,6 +741,7 @@ template <class T> struct Impl : ImplBase {
     h.ref = ref_host;
     h.dtc = pl.dtc;
     h.cur = cur;
+    h.itime0 = (int)itime_total;
   }
   int upload_ctrl(int max_steps, double tol) {
     fill_ctrl(hctrl[0], max_steps, tol);
@@ -740,6 +767,7 @@ template <class T> struct Impl : ImplBase {
     if (steps) *steps = ns;
     ref_host = c.ref;
     cur = c.cur;
+    itime_total += ns;
     if (ns > 0) {
       if (linf) CK(cudaMemcpy(linf, hist_linf, ns * sizeof(double), cudaMemcpyDeviceToHost));
       if (l2) CK(cudaMemcpy(l2, hist_l2, ns * sizeof(double), cudaMemcpyDeviceToHost));
@@ -782,7 +810,105 @@ template <class T> struct Impl : ImplBase {
     CK(cudaMemcpyAsync(&hctrl[1], ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     CK(cudaEventElapsedTime(&last_ms, ev0, ev1));
-    return collect(hctrl[1], steps, linf, l2, dt);
+    const int rc = collect(hctrl[1], steps, linf, l2, dt);
+    // the call's last step, when its record is due (the graph takes a
+    // step's record at the start of the next one)
+    if (rc == 0 && out_every > 0 && hctrl[1].step > 0 && itime_total % out_every == 0) {
+      TRY(moments_now());
+      TRY(record(out_args((int)itime_total, nullptr)));
+      CK(cudaStreamSynchronize(st));
+    }
+    return rc;
+  }
+
+  OutArgs out_args(int force_itime, double* direct) const {
+    OutArgs o{};
+    o.nod = NodalArgs{node_off, node_dg, node_ae, nraw, disux, disuy, disps, nullptr, nullptr, nullptr,
+                      nullptr, nullptr, nullptr, pl.NP, pl.M / 6.022e26, pl.rgas};
+    o.ctrl = ctrl;
+    o.fs = d_fs;
+    o.nfs = (int)pl.fsides.size();
+    o.every = out_every > 0 ? out_every : 1;
+    o.cap = out_cap > 0 ? out_cap : 1;
+    o.ring = out_ring;
+    o.count = out_count;
+    o.direct = direct;
+    o.force_itime = force_itime;
+    return o;
+  }
+  int record(const OutArgs& o) {
+    k_out_nodal<<<(pl.NP + 255) / 256, 256, 0, st>>>(o);
+    CK(cudaGetLastError());
+    k_out_forces<<<1, FORCE_THREADS, 0, st>>>(o);
+    CK(cudaGetLastError());
+    return 0;
+  }
+  size_t rec_len() const { return 4 + 6 * (size_t)pl.NP; }
+
+  int forces(double* lift, double* drag) override {
+    CK(cudaSetDevice(device));
+    if (!out_direct) TRY(dalloc(&out_direct, rec_len()));
+    TRY(moments_now());
+    TRY(record(out_args((int)itime_total, out_direct)));
+    double hdr[4];
+    CK(cudaMemcpyAsync(hdr, out_direct, sizeof hdr, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    CK(cudaMemcpy(&hctrl[1], ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost));
+    TRY(finish_status(hctrl[1]));
+    if (lift) *lift = hdr[1];
+    if (drag) *drag = hdr[2];
+    return 0;
+  }
+  int set_output(int every, int cap) override {
+    CK(cudaSetDevice(device));
+    if (every < 0 || (every > 0 && cap < 1)) {
+      set_error("dgbgk_set_output: every >= 0 and, with every > 0, capacity >= 1");
+      return DGBGK_EINVAL;
+    }
+    CK(cudaStreamSynchronize(st));
+    dfree(out_ring);
+    dfree(out_count);
+    out_every = every;
+    out_cap = every > 0 ? cap : 0;
+    if (every > 0) {
+      TRY(dalloc(&out_ring, (size_t)cap * rec_len()));
+      TRY(dalloc(&out_count, 1));
+      CK(cudaMemsetAsync(out_count, 0, sizeof(int), st));
+      CK(cudaStreamSynchronize(st));
+    }
+    drop_graphs();  // the step graph takes the record kernels or leaves them out
+    return 0;
+  }
+  int output_count(int* n) override {
+    CK(cudaSetDevice(device));
+    int c = 0;
+    if (out_count) {
+      CK(cudaMemcpyAsync(&c, out_count, sizeof(int), cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+    }
+    *n = c;
+    return 0;
+  }
+  int get_output(int k, int* itime, double* const* fields, double* lift, double* drag) override {
+    int count = 0;
+    TRY(output_count(&count));
+    const int n = std::min(count, out_cap);
+    if (k < 0 || k >= n) {
+      set_error("dgbgk_get_output: record " + std::to_string(k) + " not in the ring (" + std::to_string(n) +
+                " held)");
+      return DGBGK_EINVAL;
+    }
+    const int slot = (count - n + k) % out_cap;
+    std::vector<double> h(rec_len());
+    CK(cudaMemcpyAsync(h.data(), out_ring + (size_t)slot * rec_len(), h.size() * sizeof(double),
+                       cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (itime) *itime = (int)h[0];
+    if (lift) *lift = h[1];
+    if (drag) *drag = h[2];
+    for (int f = 0; f < 6; ++f)
+      if (fields[f]) std::memcpy(fields[f], h.data() + 4 + (size_t)f * pl.NP, pl.NP * sizeof(double));
+    return 0;
   }
 
   int profile(int nsteps, double* ms) override {
@@ -818,6 +944,7 @@ template <class T> struct Impl : ImplBase {
     CK(cudaStreamSynchronize(st));
     cur = 0;
     ++epoch;
+    itime_total = 0;  // a new state: ITIME starts again
     return 0;
   }
   int get_state(void* dst, bool f32) override {
@@ -851,6 +978,7 @@ template <class T> struct Impl : ImplBase {
     CK(cudaStreamSynchronize(st));
     cur = 0;
     ++epoch;
+    itime_total = 0;  // a new state: ITIME starts again
     return 0;
   }
   int snapshot(int slot) override {
@@ -998,6 +1126,7 @@ template <class T> struct Impl : ImplBase {
     CK(e);
     cur = 0;
     ++epoch;
+    itime_total = 0;  // a new state: ITIME starts again
     return 0;
   }
 
@@ -1023,6 +1152,7 @@ template <class T> struct Impl : ImplBase {
     CK(e);
     cur = 0;
     ++epoch;
+    itime_total = 0;  // a new state: ITIME starts again
     return 0;
   }
 
@@ -1279,11 +1409,31 @@ int dgbgk_copy_state(dgbgk_handle* dst, const dgbgk_handle* src) {
   if (rc == 0) rc = d->import_device(buf);
   cudaFree(buf);
   if (rc == 0) d->ref_host = s_->ref_host;
+  if (rc == 0) d->itime_total = s_->itime_total;
   return rc;
 }
 int dgbgk_get_macros(dgbgk_handle* h, double* nd, double* rho, double* u, double* v, double* ps, double* temp) {
   HCHECK(h);
   return h->impl->macros(nd, rho, u, v, ps, temp);
+}
+int dgbgk_get_forces(dgbgk_handle* h, double* lift, double* drag) {
+  HCHECK(h);
+  return h->impl->forces(lift, drag);
+}
+int dgbgk_set_output(dgbgk_handle* h, int every, int capacity) {
+  HCHECK(h);
+  return h->impl->set_output(every, capacity);
+}
+int dgbgk_output_count(dgbgk_handle* h, int* count) {
+  HCHECK(h);
+  if (!count) return set_error("NULL pointer"), DGBGK_EINVAL;
+  return h->impl->output_count(count);
+}
+int dgbgk_get_output(dgbgk_handle* h, int k, int* itime, double* nd, double* rho, double* u, double* v, double* ps,
+                     double* temp, double* lift, double* drag) {
+  HCHECK(h);
+  double* const fields[6] = {nd, rho, u, v, ps, temp};
+  return h->impl->get_output(k, itime, fields, lift, drag);
 }
 int dgbgk_get_node_fields(dgbgk_handle* h, double* disnd, double* disux, double* disuy, double* disps,
                           double* mu) {

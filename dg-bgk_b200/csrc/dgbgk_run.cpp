@@ -254,24 +254,6 @@ bool read_lobatto(const std::string& path, std::vector<double>& eta, std::vector
   return true;
 }
 
-// GETFOR (src/getfor.f90): pressure force on the type-4 sides
-void getfor(const Mesh& m, const std::vector<double>& ps, double& lift, double& drag) {
-  lift = drag = 0.0;
-  for (int b = 0; b < m.nboun; ++b) {
-    if (m.bsido[6 * b + 3] != 4) continue;
-    const int p1 = m.bsido[6 * b] - 1, p2 = m.bsido[6 * b + 1] - 1;
-    const double x1 = m.coord[2 * p1], y1 = m.coord[2 * p1 + 1], x2 = m.coord[2 * p2], y2 = m.coord[2 * p2 + 1];
-    const double len = std::sqrt((x2 - x1) * (x2 - x1) + (y2 - y1) * (y2 - y1));
-    double px = -(y2 - y1), py = x2 - x1;
-    const double mag = std::sqrt(px * px + py * py);
-    px /= mag;
-    py /= mag;
-    const double pav = 0.5 * (ps[p1] + ps[p2]);
-    lift -= pav * len * py;
-    drag -= pav * len * px;
-  }
-}
-
 int die(const std::string& msg) {
   std::fprintf(stderr, "dgbgk_run: %s\n", msg.c_str());
   return 1;
@@ -426,17 +408,33 @@ int main(int argc, char** argv) {
   };
   if (gather() != 0) return die(dgbgk_last_error());
   results(0);
+  // GETFOR (src/getfor.f90:29-49) on the device
   double lift = 0, drag = 0;
-  if (in.FORCEOUT != 0) getfor(m, ps, lift, drag);
+  if (in.FORCEOUT != 0 && dgbgk_get_forces(h, &lift, &drag) != 0) return die(dgbgk_last_error());
 
-  // the time loop in chunks that end where ADVNCE gathers (MOD(ITIME,1000) = 0)
+  // The time loop.  ADVNCE gathers GETMAC's fields (and GETFOR reads their
+  // PS) at MOD(ITIME,1000) = 0 (src/advnce.f90:403-435): the library records
+  // them on the device at those steps, and the driver writes them after each
+  // advance call of up to kCap such records.
+  constexpr int kEvery = 1000, kCap = 8;
+  if (dgbgk_set_output(h, kEvery, kCap) != 0) return die(dgbgk_last_error());
+  struct Rec {
+    int itime = -1;
+    double lift = 0, drag = 0;
+    std::vector<double> f[6];
+  };
+  std::vector<Rec> recs(kCap);
+  for (auto& r : recs)
+    for (auto& x : r.f) x.resize(NP);
   double sritm1 = 0;
-  int itime = 0;
+  int itime = 0, taken = 0;
   bool stopped = false;
-  std::vector<double> linf(1000), l2(1000), dte(1000);
+  std::vector<double> linf, l2, dte;
   while (itime < in.NTIME && !stopped) {
-    const int next = std::min(in.NTIME, (itime / 1000 + 1) * 1000);
-    const int n = next - itime;
+    const int n = std::min(in.NTIME - itime, kEvery * kCap);
+    linf.resize(n);
+    l2.resize(n);
+    dte.resize(n);
     int done = 0;
     const int rc = dgbgk_advance(h, n, tol, &done, linf.data(), l2.data(), dte.data());
     if (rc != 0) {
@@ -445,12 +443,31 @@ int main(int argc, char** argv) {
       std::fclose(f18);
       return die(dgbgk_last_error());
     }
+    // this call's records (at most kCap: n <= kEvery * kCap), oldest first
+    int count = 0;
+    if (dgbgk_output_count(h, &count) != 0) return die(dgbgk_last_error());
+    const int fresh = count - taken, held = std::min(count, kCap);
+    taken = count;
+    for (int r = 0; r < fresh; ++r) {
+      Rec& x = recs[r];
+      if (dgbgk_get_output(h, held - fresh + r, &x.itime, x.f[0].data(), x.f[1].data(), x.f[2].data(),
+                           x.f[3].data(), x.f[4].data(), x.f[5].data(), &x.lift, &x.drag) != 0)
+        return die(dgbgk_last_error());
+    }
+    int next = 0;
     for (int k = 0; k < done; ++k) {
       const int it = itime + k + 1;
-      if (it % 1000 == 0) {  // GETMAC before the residual line of the same step
-        if (gather() != 0) return die(dgbgk_last_error());
+      if (next < fresh && it == recs[next].itime) {  // GETMAC before the residual line of the same step
+        const Rec& x = recs[next++];
+        nd = x.f[0];
+        rho = x.f[1];
+        u = x.f[2];
+        v = x.f[3];
+        ps = x.f[4];
+        temp = x.f[5];
         results(it);
-        if (in.FORCEOUT != 0) getfor(m, ps, lift, drag);
+        lift = x.lift;
+        drag = x.drag;
       }
       const double sumres = linf[k];
       if (it == 1) sritm1 = sumres;

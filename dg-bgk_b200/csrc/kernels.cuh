@@ -1443,9 +1443,8 @@ struct NodalArgs {
   double MM, R;
 };
 
-__global__ void k_nodal(NodalArgs a) {
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= a.NP) return;
+// mesh node q's ND, RHO, UVEL, VVEL, PS, TEMP into out[k*stride + q]
+__device__ __forceinline__ void nodal_one(const NodalArgs& a, int q, double* out, int stride) {
   double flag = 0, nd = 0, u = 0, v = 0, ps = 0;
   for (int k = a.node_off[q]; k < a.node_off[q + 1]; ++k) {
     const int dg = a.node_dg[k];
@@ -1469,12 +1468,93 @@ __global__ void k_nodal(NodalArgs a) {
     ps = ps / flag;
     t = ps / (a.R * rho);
   }
-  a.nd[q] = nd;
-  a.rho[q] = rho;
-  a.u[q] = u;
-  a.v[q] = v;
-  a.ps[q] = ps;
-  a.temp[q] = t;
+  out[q] = nd;
+  out[stride + q] = rho;
+  out[2 * stride + q] = u;
+  out[3 * stride + q] = v;
+  out[4 * stride + q] = ps;
+  out[5 * stride + q] = t;
+}
+
+__global__ void k_nodal(NodalArgs a) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= a.NP) return;
+  nodal_one(a, q, a.nd, (int)(a.rho - a.nd));
+}
+
+// ------------------------------------------------ observables on device ----
+// GETMAC's nodal fields and GETFOR's lift and drag (src/getmac.f90:98-123,
+// src/getfor.f90:29-49) recorded without a host round trip.  A record is
+// [ITIME, LIFT, DRAG, 0][ND | RHO | UVEL | VVEL | PS | TEMP] (6*NPOIN).
+// Ring mode (inside the step graph, right after the moment kernel, whose
+// moments are those of the state after the previous step): the record of
+// ITIME = itime0 + step is taken when that is a multiple of `every`, into
+// slot count % cap of the ring, and count is bumped.  Direct mode
+// (force_itime >= 0): one record into `direct`, unconditionally.
+struct OutArgs {
+  NodalArgs nod;  // its nd .. temp pointers unused
+  const Ctrl* ctrl;
+  const ForceSide* fs;
+  int nfs;
+  int every, cap;
+  double* ring;   // [cap][4 + 6*NP]
+  int* count;
+  double* direct;
+  int force_itime;
+};
+__device__ __forceinline__ int out_itime(const OutArgs& o) {
+  if (o.force_itime >= 0) return o.force_itime;
+  const Ctrl* c = o.ctrl;
+  if (c->done || c->step == 0) return -1;
+  const int it = c->itime0 + c->step;
+  return (it % o.every == 0) ? it : -1;
+}
+__device__ __forceinline__ double* out_record(const OutArgs& o) {
+  if (o.direct) return o.direct;
+  return o.ring + (size_t)(*o.count % o.cap) * (4 + 6 * (size_t)o.nod.NP);
+}
+__global__ void k_out_nodal(OutArgs o) {
+  if (out_itime(o) < 0) return;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= o.nod.NP) return;
+  nodal_one(o.nod, q, out_record(o) + 4, o.nod.NP);
+}
+constexpr int FORCE_THREADS = 256;
+__global__ void __launch_bounds__(FORCE_THREADS) k_out_forces(OutArgs o) {
+  const int it = out_itime(o);
+  if (it < 0) return;
+  double* rec = out_record(o);
+  const double* ps = rec + 4 + 4 * (size_t)o.nod.NP;
+  double lift = 0.0, drag = 0.0;
+  for (int k = threadIdx.x; k < o.nfs; k += FORCE_THREADS) {
+    const ForceSide s = o.fs[k];
+    const double pav = 0.5 * (ps[s.ip1] + ps[s.ip2]);
+    lift -= pav * s.ly;
+    drag -= pav * s.lx;
+  }
+  __shared__ double red[2][FORCE_THREADS / 32];
+  lift = warp_sum(lift);
+  drag = warp_sum(drag);
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = lift;
+    red[1][threadIdx.x >> 5] = drag;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double l = 0.0, d = 0.0;
+    for (int w = 0; w < FORCE_THREADS / 32; ++w) {
+      l += red[0][w];
+      d += red[1][w];
+    }
+    rec[0] = (double)it;
+    rec[1] = l;
+    rec[2] = d;
+    rec[3] = 0.0;
+    if (!o.direct) {
+      __threadfence();
+      *o.count += 1;
+    }
+  }
 }
 
 // ---------------------------------------------- vector extrapolation ----

@@ -402,6 +402,23 @@ int build_plan(const dgbgk_mesh& m, const dgbgk_vspace& vs, const dgbgk_params& 
   for (int s = S - 1; s >= 0; --s) {
     sfind[{m.iside[8 * s], m.iside[8 * s + 1]}] = s;
   }
+  // GETFOR's sides (src/getfor.f90:29-49): LEN and the rotated unit normal
+  // PERP from the node coordinates, in FP64
+  pl.fsides.clear();
+  for (int b = 0; b < B; ++b) {
+    if (m.bsido[6 * b + 3] != 4) continue;
+    const int ip1 = m.bsido[6 * b] - 1, ip2 = m.bsido[6 * b + 1] - 1;
+    if (ip1 < 0 || ip1 >= NP || ip2 < 0 || ip2 >= NP)
+      return fail(DGBGK_EMESH, "dgbgk_create: BSIDO node outside 1..NPOIN");
+    const double x1 = m.coord[2 * ip1], y1 = m.coord[2 * ip1 + 1], x2 = m.coord[2 * ip2], y2 = m.coord[2 * ip2 + 1];
+    const double len = std::sqrt((x2 - x1) * (x2 - x1) + (y2 - y1) * (y2 - y1));
+    double px = -(y2 - y1), py = x2 - x1;  // ROTMAT * VEC
+    const double mag = std::sqrt(px * px + py * py);
+    if (!(mag > 0.0)) return fail(DGBGK_EMESH, "dgbgk_create: zero-length wall side (GETFOR)");
+    px /= mag;
+    py /= mag;
+    pl.fsides.push_back(ForceSide{ip1, ip2, len * px, len * py});
+  }
   pl.walls.clear();
   for (int b = 0; b < B; ++b) {
     if (m.bsido[6 * b + 3] != 4) continue;

@@ -46,6 +46,7 @@ struct Plan {
   // boundary sides
   std::vector<double> bTw, bUw;  // [B], [2B]
   std::vector<WallSide> walls;   // type-4 sides (FLUCON2)
+  std::vector<ForceSide> fsides; // type-4 sides in boundary-side order (GETFOR)
   bool has_wall_incoming = false;  // some side of a kind-3 wall exists
   // nodal gather (MACROS tail / GETMAC): CSR over mesh nodes
   std::vector<int> node_off, node_dg;  // DG node index (plan order) per entry

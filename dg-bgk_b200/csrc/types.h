@@ -83,6 +83,14 @@ struct WallSide {
   double sumbottom;    // sqrt(2*PI*R^3*T_w^3)
 };
 
+// One type-4 wall side for GETFOR's lift and drag (src/getfor.f90:29-49):
+// its two nodes and LEN*PERP, PERP the unit normal of the side vector
+// turned 90 degrees anticlockwise.
+struct ForceSide {
+  int ip1, ip2;  // nodes BSIDO(1), BSIDO(2), 0-based
+  double lx, ly; // LEN*PERP(1), LEN*PERP(2)
+};
+
 // Device-side control block of one case.
 struct Ctrl {
   int done;       // kernels skip the case when set
@@ -97,6 +105,8 @@ struct Ctrl {
   double acc_max; // max residual of the current step (atomicMax on the bits; reset by k_resid)
   int cur;        // which f buffer holds the current state (k_resid swaps it)
   int timeout;    // set when a bounded device wait gave up
+  int itime0;     // steps the handle ran before this advance call (the reference's ITIME - step - 1)
+  int pad0;
 };
 
 // Device-side control of one launch set (a case alone or a batch).

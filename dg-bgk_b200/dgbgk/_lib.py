@@ -78,6 +78,10 @@ SIGNATURES = {
     "dgbgk_extrapolate": (c_int, [c_void_p, c_int, _PD]),
     "dgbgk_get_macros": (c_int, [c_void_p, _PD, _PD, _PD, _PD, _PD, _PD]),
     "dgbgk_get_macros_noalloc": (c_int, [c_void_p, _PD, _PD, _PD, _PD, _PD, _PD]),
+    "dgbgk_get_forces": (c_int, [c_void_p, _PD, _PD]),
+    "dgbgk_set_output": (c_int, [c_void_p, c_int, c_int]),
+    "dgbgk_output_count": (c_int, [c_void_p, _PI]),
+    "dgbgk_get_output": (c_int, [c_void_p, c_int, _PI, _PD, _PD, _PD, _PD, _PD, _PD, _PD, _PD]),
     "dgbgk_get_node_fields": (c_int, [c_void_p, _PD, _PD, _PD, _PD, _PD]),
     "dgbgk_get_wall_eta": (c_int, [c_void_p, _PD]),
     "dgbgk_info": (c_int, [c_void_p, _PI]),

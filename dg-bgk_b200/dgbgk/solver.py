@@ -157,8 +157,15 @@ class Solver:
             assert a.size == 3 * self.E * self.V
             check(lib().dgbgk_set_state(self.h, ptr(a)))
 
-    def get_state(self, dtype=np.float64):
-        out = np.empty((self.E, self.V, 3), dtype=dtype)
+    def get_state(self, dtype=np.float64, out=None):
+        """DISNF as (NELEM, VNPNT, 3); into `out` when given (a C-contiguous
+        array of that shape and dtype, e.g. a pinned host buffer: the device
+        copy lands in it directly)."""
+        if out is None:
+            out = np.empty((self.E, self.V, 3), dtype=dtype)
+        else:
+            dtype = out.dtype.type
+            assert out.shape == (self.E, self.V, 3) and out.flags["C_CONTIGUOUS"]
         if dtype == np.float32:
             check(lib().dgbgk_get_state_f32(self.h, ptr(out, c_float)))
         else:
@@ -234,6 +241,34 @@ class Solver:
     def macros(self):
         out = {k: np.zeros(self.NP) for k in ("nd", "rho", "u", "v", "ps", "temp")}
         check(lib().dgbgk_get_macros(self.h, *(ptr(out[k]) for k in ("nd", "rho", "u", "v", "ps", "temp"))))
+        return out
+
+    def forces(self):
+        """GETFOR's (lift, drag) of the current state, reduced on the device."""
+        lift, drag = c_double(0), c_double(0)
+        check(lib().dgbgk_get_forces(self.h, ctypes.byref(lift), ctypes.byref(drag)))
+        return lift.value, drag.value
+
+    def set_output(self, every, capacity=16):
+        """Record GETMAC's nodal fields and GETFOR's forces every `every`
+        steps of advance() into a device ring (every = 0: stop)."""
+        check(lib().dgbgk_set_output(self.h, every, capacity))
+        self._out_cap = capacity if every > 0 else 0
+
+    def outputs(self):
+        """The records held by the ring, oldest first: dicts of itime, lift,
+        drag and the six nodal fields."""
+        n = c_int(0)
+        check(lib().dgbgk_output_count(self.h, ctypes.byref(n)))
+        out = []
+        keys = ("nd", "rho", "u", "v", "ps", "temp")
+        for k in range(min(n.value, getattr(self, "_out_cap", 0))):
+            f = {key: np.zeros(self.NP) for key in keys}
+            it, lift, drag = c_int(0), c_double(0), c_double(0)
+            check(lib().dgbgk_get_output(self.h, k, ctypes.byref(it), *(ptr(f[key]) for key in keys),
+                                         ctypes.byref(lift), ctypes.byref(drag)))
+            f.update(itime=it.value, lift=lift.value, drag=drag.value)
+            out.append(f)
         return out
 
     def node_fields(self):

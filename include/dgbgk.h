@@ -169,6 +169,28 @@ int dgbgk_copy_state(dgbgk_handle* dst, const dgbgk_handle* src);
 int dgbgk_snapshot(dgbgk_handle* h, int slot);
 int dgbgk_extrapolate(dgbgk_handle* h, int n, double* gamma);
 
+/* GETFOR (src/getfor.f90:29-49) of the current state: the lift and drag
+ * of the type-4 wall sides from the nodal pressure, reduced on the device
+ * after MACROS + GETMAC; two numbers cross to the host. */
+int dgbgk_get_forces(dgbgk_handle* h, double* lift, double* drag);
+
+/* ADVNCE's periodic output (src/advnce.f90:403-417, GETFOR at :427-435)
+ * without a host round trip: with every > 0, dgbgk_advance records GETMAC's
+ * nodal fields (ND, RHO, UVEL, VVEL, PS, TEMP) and GETFOR's lift and drag
+ * whenever ITIME -- the steps the handle has run since its state was last
+ * set (dgbgk_set_state*, dgbgk_init_*), counted across advance calls and
+ * carried over by dgbgk_copy_state -- is a multiple of `every`, into a
+ * device ring of `capacity` records (the oldest is overwritten).  Each call
+ * replaces the ring; every = 0 stops recording.  Batches do not record. */
+int dgbgk_set_output(dgbgk_handle* h, int every, int capacity);
+/* Records taken since dgbgk_set_output (the ring holds the last
+ * min(count, capacity)). */
+int dgbgk_output_count(dgbgk_handle* h, int* count);
+/* Record k of those held (0 = the oldest): its ITIME, the six nodal fields
+ * (NPOIN values each) and lift and drag; any pointer may be NULL. */
+int dgbgk_get_output(dgbgk_handle* h, int k, int* itime, double* nd, double* rho, double* u, double* v, double* ps,
+                     double* temp, double* lift, double* drag);
+
 /* MACROS (src/macros.f90:51-188) + GETMAC (src/getmac.f90:98-123) of the
  * current state: nodal ND, RHO, UVEL, VVEL, PS, TEMP, NPOIN values each. */
 int dgbgk_get_macros(dgbgk_handle* h, double* nd, double* rho, double* u, double* v, double* ps,

@@ -104,6 +104,13 @@ struct ImplBase {
   float last_ms = 0.f;
   int mom_rows_req = 0;  // moment rows per warp step asked for at create (0: the heuristic)
   long long itime_total = 0;  // steps run since the state was last set (the reference's ITIME)
+  bool shard = false;         // a velocity shard: its steps run through the shard phases
+  // velocity-shard step phases (the caller sums the partials between them)
+  virtual int shard_begin(int max_steps, double tol) = 0;
+  virtual int shard_phase(int k, double* sums1, double* sums2, double* res) = 0;
+  virtual int shard_end(int* steps, double* linf, double* l2, double* dt, int* done) = 0;
+  virtual void* stream_ptr() = 0;
+  virtual int shard_poll(int* done) = 0;
   // bumped when the case's device table entry changes (buffers moved,
   // re-blocked): a batch holding the case rebuilds its table
   unsigned gen = 0;
@@ -776,7 +783,72 @@ template <class T> struct Impl : ImplBase {
     return finish_status(c);
   }
 
+  // Velocity shard: one step in four phases on the handle's stream,
+  //   1: pass-1 partial sums -> sums1;
+  //   2: pass-2 partial sums with the summed sums1 -> sums2 (+ the walls);
+  //   3: moments, MU, parameters, ETA from the summed sums; the sweep of the
+  //      shard's velocities; residual partials -> res;
+  //   4: the step's bookkeeping with the reduced res;
+  // the caller sums sums1 and sums2 and takes the max (res[0]) and sum
+  // (res[1]) over the shards between them, on this stream.
+  int shard_begin(int max_steps, double tol) override {
+    CK(cudaSetDevice(device));
+    TRY(ensure_hist(std::max(max_steps, 1)));
+    TRY(upload_ctrl(max_steps, tol));
+    CK(cudaEventRecord(ev0, st));
+    return 0;
+  }
+  int shard_phase(int k, double* sums1, double* sums2, double* res) override {
+    const int n3 = 3 * pl.E;
+    const int gw = (n3 * 32 + 255) / 256;  // a warp per DG node
+    const CaseDev<T>& C = single.one_case;
+    if (k == 1) {
+      k_shard_sums1<T><<<gw, 256, 0, st>>>(C, sums1);
+    } else if (k == 2) {
+      k_shard_sums2<T><<<gw, 256, 0, st>>>(C, sums1, sums2);
+      if (single.total_walls > 0) k_shard_wall<T><<<single.total_walls, WALL_THREADS, 0, st>>>(C, sums2 + 2 * (size_t)n3);
+    } else if (k == 3) {
+      const int nt = std::max(n3, (int)pl.walls.size());
+      k_shard_fin<T><<<(nt + 255) / 256, 256, 0, st>>>(C, sums1, sums2);
+      constexpr int TPE = SweepGeo<T>::TPE;
+      sweep_fn<T>(single.eb, single.immat, true)<<<single.sweep_grid, TPE * single.eb, single.sweep_smem, st>>>(
+          single.args, single.total_units, single.one_case);
+      k_shard_respart<T><<<1, 32, 0, st>>>(C, res);
+    } else if (k == 4) {
+      k_shard_resid<T><<<1, 32, 0, st>>>(C, res, single.args.ctl);
+    } else if (k == 0) {  // before phases 1, 2 and 5 outside a step: the kernels run
+      TRY(aux_ctrl());
+    } else if (k == 5) {  // the moments of the current state from the summed sums (no sweep)
+      const int nt = std::max(n3, (int)pl.walls.size());
+      k_shard_fin<T><<<(nt + 255) / 256, 256, 0, st>>>(C, sums1, sums2);
+    } else {
+      set_error("dgbgk_shard_phase: phase 0 to 5");
+      return DGBGK_EINVAL;
+    }
+    CK(cudaGetLastError());
+    return 0;
+  }
+  int shard_end(int* steps, double* linf, double* l2, double* dt, int* done) override {
+    CK(cudaEventRecord(ev1, st));
+    CK(cudaMemcpyAsync(&hctrl[1], ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    CK(cudaEventElapsedTime(&last_ms, ev0, ev1));
+    if (done) *done = hctrl[1].done;
+    return collect(hctrl[1], steps, linf, l2, dt);
+  }
+  void* stream_ptr() override { return (void*)st; }
+  int shard_poll(int* done) override {
+    CK(cudaMemcpyAsync(&hctrl[2], ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    *done = hctrl[2].done;
+    return 0;
+  }
+
   int advance(int max_steps, double tol, int* steps, double* linf, double* l2, double* dt) override {
+    if (shard) {
+      set_error("dgbgk_advance: a velocity shard steps through dgbgk_shard_*");
+      return DGBGK_EINVAL;
+    }
     if (max_steps < 0) {
       set_error("max_steps < 0");
       return DGBGK_EINVAL;
@@ -1156,7 +1228,10 @@ template <class T> struct Impl : ImplBase {
     return 0;
   }
 
+  // the moments of the current state (a velocity shard has them from its
+  // last phase 3 or 5: the sums are over every shard)
   int moments_now() {
+    if (shard) return 0;
     TRY(aux_ctrl());
     mom_fn<T>(single.mom_rows, true)<<<single.mom_grid, single.mom_warps * 32, single.mom_smem, st>>>(
         single.args, single.total_groups, single.one_case);
@@ -1313,6 +1388,11 @@ int dgbgk_create(const dgbgk_mesh* mesh, const dgbgk_vspace* vs, const dgbgk_par
     return DGBGK_EINVAL;
   }
   impl->mom_rows_req = prm->moment_rows;
+  impl->shard = prm->shard != 0;
+  if (impl->shard && prm->alpha < 1.0) {
+    set_error("dgbgk_create: a velocity shard needs ALPHA = 1 (the specular part reads mirrored velocities)");
+    return DGBGK_EUNSUP;
+  }
   std::string err;
   const int eb0 = prm->tile_elems > 0      ? prm->tile_elems
                   : prm->precision == 64 ? Impl<double>::default_eb()
@@ -1422,6 +1502,7 @@ int dgbgk_get_forces(dgbgk_handle* h, double* lift, double* drag) {
 }
 int dgbgk_set_output(dgbgk_handle* h, int every, int capacity) {
   HCHECK(h);
+  if (h->impl->shard) return set_error("dgbgk_set_output: not for a velocity shard"), DGBGK_EINVAL;
   return h->impl->set_output(every, capacity);
 }
 int dgbgk_output_count(dgbgk_handle* h, int* count) {
@@ -1461,6 +1542,45 @@ int dgbgk_profile_steps(dgbgk_handle* h, int nsteps, double* kernel_ms) {
   HCHECK(h);
   if (!kernel_ms || nsteps < 1) return set_error("bad arguments"), DGBGK_EINVAL;
   return h->impl->profile(nsteps, kernel_ms);
+}
+#define SCHECK(h)                                                                   \
+  do {                                                                              \
+    HCHECK(h);                                                                      \
+    if (!(h)->impl->shard) return set_error("not a velocity shard"), DGBGK_EINVAL; \
+  } while (0)
+int dgbgk_shard_stream(dgbgk_handle* h, void** stream) {
+  SCHECK(h);
+  if (!stream) return set_error("NULL pointer"), DGBGK_EINVAL;
+  *stream = h->impl->stream_ptr();
+  return 0;
+}
+int dgbgk_shard_sizes(dgbgk_handle* h, long long* n_sums1, long long* n_sums2) {
+  SCHECK(h);
+  const long long n3 = 3LL * h->impl->pl.E;
+  if (n_sums1) *n_sums1 = 3 * n3;
+  if (n_sums2) *n_sums2 = 2 * n3 + (long long)h->impl->pl.walls.size();
+  return 0;
+}
+int dgbgk_shard_begin(dgbgk_handle* h, int max_steps, double tol) {
+  SCHECK(h);
+  if (max_steps < 1) return set_error("dgbgk_shard_begin: max_steps >= 1"), DGBGK_EINVAL;
+  return h->impl->shard_begin(max_steps, tol);
+}
+int dgbgk_shard_phase(dgbgk_handle* h, int phase, double* sums1, double* sums2, double* res) {
+  SCHECK(h);
+  if ((phase >= 1 && phase != 4 && !sums1) || ((phase == 2 || phase == 3 || phase == 5) && !sums2) ||
+      ((phase == 3 || phase == 4) && !res))
+    return set_error("dgbgk_shard_phase: NULL exchange buffer"), DGBGK_EINVAL;
+  return h->impl->shard_phase(phase, sums1, sums2, res);
+}
+int dgbgk_shard_poll(dgbgk_handle* h, int* done) {
+  SCHECK(h);
+  if (!done) return set_error("NULL pointer"), DGBGK_EINVAL;
+  return h->impl->shard_poll(done);
+}
+int dgbgk_shard_end(dgbgk_handle* h, int* steps_done, double* res_linf, double* res_l2, double* dte, int* done) {
+  SCHECK(h);
+  return h->impl->shard_end(steps_done, res_linf, res_l2, dte, done);
 }
 void dgbgk_destroy(dgbgk_handle* h) { delete h; }
 
@@ -1811,11 +1931,16 @@ int dgbgk_batch_create(dgbgk_handle* const* cases, int ncases, const dgbgk_batch
   dgbgk_batch_default_params(&p);
   if (prm) p = *prm;
   const int prec = cases[0] && cases[0]->impl ? cases[0]->impl->prec : 0;
-  for (int i = 0; i < ncases; ++i)
+  for (int i = 0; i < ncases; ++i) {
     if (!cases[i] || !cases[i]->impl || cases[i]->impl->prec != prec) {
       set_error("dgbgk_batch_create: NULL handle or mixed precision");
       return DGBGK_EINVAL;
     }
+    if (cases[i]->impl->shard) {
+      set_error("dgbgk_batch_create: a velocity shard steps through dgbgk_shard_*");
+      return DGBGK_EINVAL;
+    }
+  }
   for (int i = 0; i < ncases; ++i)
     for (int k = 0; k < i; ++k)
       if (cases[i] == cases[k]) {

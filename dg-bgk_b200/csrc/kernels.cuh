@@ -398,6 +398,51 @@ template <> struct ElemMath<double> {
   }
 };
 
+// MACROS / COMPMU / GTEQNF per DG node from its velocity sums
+// (src/macros.f90:126-154, src/compmu.f90:86-97, src/gteqnf.f90:28-37):
+// s0 = n (before the 1e-20 test), (ux, uy), nd = n or 0, sp = the pressure
+// sum over M/NA, sc = the mean-relative-speed sum; writes the node's
+// moments, MU and the sweep's NFO parameters, returns MU.
+template <class T>
+__device__ __forceinline__ double node_epilogue(const CaseDev<T>& C, int node, double s0, double ux, double uy,
+                                                double nd, double sp, double sc) {
+  const double ps = sp * C.MM;
+  const double ct = (nd >= TINY_D) ? sc / nd : 0.0;
+  const double mu = sqrt(2.0) * ct * C.sigt * nd;
+  const int e = node / 3, i = node - 3 * (node / 3);
+  ElemRec<T>& en = C.rec[e];
+  // GTEQNF's parameters; FP64 in the expanded exponent form of the sweep
+  // (ElemRec)
+  if (ps >= TINY_D) {
+    const double rho = C.MM * nd;
+    const double b2 = rho / (2 * ps);
+    const double a = nd * (b2 / PI_D);
+    if (sizeof(T) == 4) {
+      en.A[i] = (T)a;
+      en.ex[i] = (T)(-b2 * LOG2E_D);
+      en.ux[i] = (T)ux;
+      en.uy[i] = (T)uy;
+    } else {
+      en.A[i] = (T)(log(a) - b2 * (ux * ux + uy * uy));
+      en.ex[i] = (T)(-b2);
+      en.ux[i] = (T)(2.0 * b2 * ux);
+      en.uy[i] = (T)(2.0 * b2 * uy);
+    }
+  } else {
+    en.A[i] = (T)(sizeof(T) == 4 ? 0.0 : -INFINITY);
+    en.ex[i] = (T)0;
+    en.ux[i] = (T)(sizeof(T) == 4 ? ux : 0.0);
+    en.uy[i] = (T)(sizeof(T) == 4 ? uy : 0.0);
+  }
+  en.mu[i] = (T)mu;
+  C.nraw[node] = s0;
+  C.disux[node] = ux;
+  C.disuy[node] = uy;
+  C.disps[node] = ps;
+  C.mu[node] = mu;
+  return mu;
+}
+
 // Sum over the L lanes of an aligned lane group (every lane gets the same
 // bits: each butterfly level adds the same two operands in either order).
 template <int L> __device__ __forceinline__ double group_sum(double v) {
@@ -555,43 +600,7 @@ __global__ void __launch_bounds__(ONE ? 640 : 512, 1)
         fill(s, nxt);
       }
     }
-    if ((ELEM ? lane < 3 : sub == 0) && live) {
-      const double ps = sp * C.MM;
-      const double ct = (nd >= TINY_D) ? sc / nd : 0.0;
-      const double mu = sqrt(2.0) * ct * C.sigt * nd;
-      const int e = node / 3, i = node - 3 * (node / 3);
-      ElemRec<T>& en = C.rec[e];
-      // GTEQNF's parameters (src/gteqnf.f90:28-37); FP64 in the expanded
-      // exponent form of the sweep (ElemRec)
-      if (ps >= TINY_D) {
-        const double rho = C.MM * nd;
-        const double b2 = rho / (2 * ps);
-        const double a = nd * (b2 / PI_D);
-        if (sizeof(T) == 4) {
-          en.A[i] = (T)a;
-          en.ex[i] = (T)(-b2 * LOG2E_D);
-          en.ux[i] = (T)ux;
-          en.uy[i] = (T)uy;
-        } else {
-          en.A[i] = (T)(log(a) - b2 * (ux * ux + uy * uy));
-          en.ex[i] = (T)(-b2);
-          en.ux[i] = (T)(2.0 * b2 * ux);
-          en.uy[i] = (T)(2.0 * b2 * uy);
-        }
-      } else {
-        en.A[i] = (T)(sizeof(T) == 4 ? 0.0 : -INFINITY);
-        en.ex[i] = (T)0;
-        en.ux[i] = (T)(sizeof(T) == 4 ? ux : 0.0);
-        en.uy[i] = (T)(sizeof(T) == 4 ? uy : 0.0);
-      }
-      en.mu[i] = (T)mu;
-      C.nraw[node] = s0;
-      C.disux[node] = ux;
-      C.disuy[node] = uy;
-      C.disps[node] = ps;
-      C.mu[node] = mu;
-      mumax = fmax(mumax, mu);
-    }
+    if ((ELEM ? lane < 3 : sub == 0) && live) mumax = fmax(mumax, node_epilogue(C, node, s0, ux, uy, nd, sp, sc));
     s = (s + 1 == nstage) ? 0 : s + 1;
   }
   if (aborted) {
@@ -1401,13 +1410,8 @@ template <class T> __global__ void __launch_bounds__(256) k_wspec(const __grid_c
 // one thread per case: the step's max and L2 residual into the history, the
 // non-finite and convergence tests, the step counter and the buffer swap;
 // the step's accumulators are cleared for the next step.
-template <class T> __global__ void k_resid(BatchArgs<T> a) {
-  if (threadIdx.x != 0) return;
-  if (blockIdx.x == 0) a.ctl->sweep_next = 0;
-  const CaseDev<T>& C = a.cases[blockIdx.x];
+template <class T> __device__ __forceinline__ void resid_book(const CaseDev<T>& C, double mm, double sq) {
   Ctrl* c = C.ctrl;
-  if (c->done) return;
-  const double mm = c->acc_max, sq = c->acc_sq;
   const int st = c->step;
   const double l2 = sqrt(sq);
   C.hist_linf[st] = mm;
@@ -1426,6 +1430,136 @@ template <class T> __global__ void k_resid(BatchArgs<T> a) {
   c->step = st + 1;
   if (c->step >= c->max_steps) c->done = 1;
   if (c->tol > 0.0 && l2 <= c->tol * c->ref) c->done = 1;
+}
+template <class T> __global__ void k_resid(BatchArgs<T> a) {
+  if (threadIdx.x != 0) return;
+  if (blockIdx.x == 0) a.ctl->sweep_next = 0;
+  const CaseDev<T>& C = a.cases[blockIdx.x];
+  if (C.ctrl->done) return;
+  resid_book(C, C.ctrl->acc_max, C.ctrl->acc_sq);
+}
+
+// ------------------------------------------------- velocity-space shards ----
+// A handle that holds only some speed rings of the velocity grid (the
+// reference's V-communicator partition, src/spectralbgk.f90:163-199)
+// forms partial velocity sums; the caller adds them up over the shards
+// between the phases of a step, as the reference's MPI_ALLREDUCEs over
+// MPI_COMM_V do (src/macros.f90:114-119, 153-154; src/compmu.f90:80-81;
+// src/flucon2.f90:215-216).  Exchange buffers (device, the caller's):
+//   sums1 [3][3E]: n, n*ux, n*uy per DG node (MACROS pass 1);
+//   sums2 [2][3E] + [nwall]: the pressure sum over M/NA, COMPMU's mean
+//          relative-speed sum, FLUCON2's wall sums;
+//   res [2]: the step's max residual and sum of squared changes.
+// One warp per DG node (a row of f in global memory, 16-byte vectors).
+template <class T>
+__global__ void __launch_bounds__(256) k_shard_sums1(const __grid_constant__ CaseDev<T> C, double* __restrict__ sums1) {
+  if (C.ctrl->done) return;
+  const int lane = threadIdx.x & 31, node = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (node >= 3 * C.E) return;
+  const T* row = C.f[C.ctrl->cur] + (size_t)node * C.Vp;
+  double s0 = 0, s1 = 0, s2 = 0;
+  RowMath<T>::pass1(row, C.tabs, C.Vp, (int)(C.rowbytes / 16), lane, 32, s0, s1, s2);
+  s0 = group_sum<32>(s0);
+  s1 = group_sum<32>(s1);
+  s2 = group_sum<32>(s2);
+  if (lane == 0) {
+    const size_t n3 = 3 * (size_t)C.E;
+    sums1[node] = s0;
+    sums1[n3 + node] = s1;
+    sums1[2 * n3 + node] = s2;
+  }
+}
+// the bulk velocity of a node from the summed pass-1 sums (src/macros.f90:126-134)
+__device__ __forceinline__ void shard_u(const double* __restrict__ sums1, size_t n3, int node, double& s0,
+                                        double& ux, double& uy) {
+  s0 = sums1[node];
+  ux = uy = 0.0;
+  if (s0 >= TINY_D) {
+    ux = sums1[n3 + node] / s0;
+    uy = sums1[2 * n3 + node] / s0;
+  }
+}
+template <class T>
+__global__ void __launch_bounds__(256) k_shard_sums2(const __grid_constant__ CaseDev<T> C,
+                                                     const double* __restrict__ sums1, double* __restrict__ sums2) {
+  if (C.ctrl->done) return;
+  const int lane = threadIdx.x & 31, node = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (node >= 3 * C.E) return;
+  const size_t n3 = 3 * (size_t)C.E;
+  double s0, ux, uy;
+  shard_u(sums1, n3, node, s0, ux, uy);
+  const T* row = C.f[C.ctrl->cur] + (size_t)node * C.Vp;
+  double sp = 0, sc = 0;
+  RowMath<T>::pass2(row, C.tabs, C.Vp, (int)(C.rowbytes / 16), lane, 32, ux, uy, sp, sc);
+  sp = group_sum<32>(sp);
+  sc = group_sum<32>(sc);
+  if (lane == 0) {
+    sums2[node] = sp;
+    sums2[n3 + node] = sc;
+  }
+}
+// FLUCON2's sum over this shard's outgoing velocities, one CTA per wall side
+template <class T>
+__global__ void __launch_bounds__(WALL_THREADS) k_shard_wall(const __grid_constant__ CaseDev<T> C,
+                                                             double* __restrict__ wsum) {
+  __shared__ double part[WALL_THREADS / 32];
+  if (C.ctrl->done) return;
+  const WallSide ws = C.walls[blockIdx.x];
+  const T* f = C.f[C.ctrl->cur];
+  const T* f1 = f + ((size_t)ws.elem * 3 + ws.in1) * C.Vp;
+  const T* f2 = f + ((size_t)ws.elem * 3 + ws.in2) * C.Vp;
+  double t = 0;
+  for (int v = threadIdx.x; v < C.V; v += WALL_THREADS) {
+    const double test = C.cxD[v] * ws.anx + C.cyD[v] * ws.any;
+    if (test > 0.0) t += fabs(test) * (0.5 * ((double)f1[v] + (double)f2[v])) * C.wjf[v];
+  }
+  t = warp_sum(t);
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = t;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double u = 0;
+#pragma unroll
+    for (int k = 0; k < WALL_THREADS / 32; ++k) u += part[k];
+    wsum[blockIdx.x] = u;
+  }
+}
+// the nodes' moments, MU and NFO parameters and the walls' ETA from the
+// summed partials
+template <class T>
+__global__ void __launch_bounds__(256) k_shard_fin(const __grid_constant__ CaseDev<T> C,
+                                                   const double* __restrict__ sums1, const double* __restrict__ sums2) {
+  if (C.ctrl->done) return;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t n3 = 3 * (size_t)C.E;
+  double mu = 0.0;
+  if (t < (int)n3) {
+    double s0, ux, uy;
+    shard_u(sums1, n3, t, s0, ux, uy);
+    mu = node_epilogue(C, t, s0, ux, uy, s0 >= TINY_D ? s0 : 0.0, sums2[t], sums2[n3 + t]);
+  }
+  if (t < C.nwall) {
+    const WallSide ws = C.walls[t];
+    const double eta = sums2[2 * n3 + t] / ws.sumbottom;
+    C.bEtaD[ws.bside] = eta;
+    C.bEta[ws.bside] = (T)eta;
+  }
+  const double m = warp_max(mu);
+  if ((threadIdx.x & 31) == 0 && m > 0.0)
+    atomicMax(reinterpret_cast<unsigned long long*>(&C.ctrl->maxmu), (unsigned long long)__double_as_longlong(m));
+}
+// the step's residual partials out; after the sum / max over the shards,
+// the bookkeeping of k_resid with the global values
+template <class T> __global__ void k_shard_respart(const __grid_constant__ CaseDev<T> C, double* __restrict__ res) {
+  if (threadIdx.x != 0 || C.ctrl->done) return;
+  res[0] = C.ctrl->acc_max;
+  res[1] = C.ctrl->acc_sq;
+}
+template <class T>
+__global__ void k_shard_resid(const __grid_constant__ CaseDev<T> C, const double* __restrict__ res, BatchCtl* ctl) {
+  if (threadIdx.x != 0) return;
+  ctl->sweep_next = 0;
+  if (C.ctrl->done) return;
+  resid_book(C, res[0], res[1]);
 }
 
 // -------------------------------------------------------------- nodal ----

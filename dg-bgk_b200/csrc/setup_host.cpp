@@ -31,6 +31,7 @@ extern "C" void dgbgk_default_params(dgbgk_params* p) {
   p->wall_velocity = nullptr;
   p->tile_elems = 0;
   p->moment_rows = 0;
+  p->shard = 0;
   p->device = 0;
 }
 

@@ -47,7 +47,7 @@ class Params(ctypes.Structure):
         ("immat", c_int), ("csafm", c_double), ("alpha", c_double), ("rgas", c_double),
         ("molar_mass", c_double), ("diameter", c_double), ("cinf", c_double * 4),
         ("precision", c_int), ("wall_velocity", POINTER(c_double)),
-        ("tile_elems", c_int), ("moment_rows", c_int), ("device", c_int),
+        ("tile_elems", c_int), ("moment_rows", c_int), ("device", c_int), ("shard", c_int),
     ]
 
 
@@ -83,6 +83,12 @@ SIGNATURES = {
     "dgbgk_output_count": (c_int, [c_void_p, _PI]),
     "dgbgk_get_output": (c_int, [c_void_p, c_int, _PI, _PD, _PD, _PD, _PD, _PD, _PD, _PD, _PD]),
     "dgbgk_get_node_fields": (c_int, [c_void_p, _PD, _PD, _PD, _PD, _PD]),
+    "dgbgk_shard_stream": (c_int, [c_void_p, POINTER(c_void_p)]),
+    "dgbgk_shard_sizes": (c_int, [c_void_p, POINTER(ctypes.c_longlong), POINTER(ctypes.c_longlong)]),
+    "dgbgk_shard_begin": (c_int, [c_void_p, c_int, c_double]),
+    "dgbgk_shard_phase": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
+    "dgbgk_shard_poll": (c_int, [c_void_p, _PI]),
+    "dgbgk_shard_end": (c_int, [c_void_p, _PI, _PD, _PD, _PD, _PI]),
     "dgbgk_get_wall_eta": (c_int, [c_void_p, _PD]),
     "dgbgk_info": (c_int, [c_void_p, _PI]),
     "dgbgk_last_timing": (c_int, [c_void_p, _PD]),

@@ -69,7 +69,7 @@ class Solver:
 
     def __init__(self, intma, coord, bsido, setup, vcord, sumweight, rorder, torder, rv, *, immat=1, csafm=0.5,
                  alpha=1.0, rgas=1.0, molar_mass=6.022e26, diameter=1.0, cinf=(0, 0, 0, 0), precision=64,
-                 wall_velocity=None, tile_elems=0, moment_rows=0, device=0):
+                 wall_velocity=None, tile_elems=0, moment_rows=0, device=0, shard=0):
         L = lib()
         self._keep = []
 
@@ -113,6 +113,7 @@ class Solver:
         p.tile_elems = tile_elems
         p.moment_rows = moment_rows
         p.device = device
+        p.shard = shard
         h = c_void_p()
         check(L.dgbgk_create(ctypes.byref(m), ctypes.byref(vs), ctypes.byref(p), ctypes.byref(h)))
         self.h = h

@@ -88,6 +88,10 @@ typedef struct dgbgk_params {
                          three rows of one element on all 32 lanes (0 = the
                          library's choice) */
   int device;         /* CUDA device ordinal                               */
+  int shard;          /* 1: the handle holds a velocity shard -- the vspace
+                         passed has only its speed rings (RORDER = their
+                         count), with the full grid's SUMWEIGHT -- and its
+                         steps run through dgbgk_shard_* (0 = whole grid) */
 } dgbgk_params;
 
 /* Fills a dgbgk_params with the reference defaults of
@@ -235,6 +239,36 @@ int dgbgk_profile_steps(dgbgk_handle* h, int nsteps, double* kernel_ms);
 #define DGBGK_NOALLOC_MAX_NPOIN 131072
 int dgbgk_get_macros_noalloc(dgbgk_handle* h, double* nd, double* rho, double* u, double* v, double* ps,
                              double* temp);
+
+/* ---- Velocity-space shards ----------------------------------------------
+ * The reference splits velocity space into NVSPACEPART blocks of whole speed
+ * rings (src/spectralbgk.f90:163-199) and sums the partial velocity sums of
+ * MACROS, COMPMU and FLUCON2 over them with MPI_ALLREDUCE
+ * (src/macros.f90:114-119, 153-154; src/compmu.f90:80-81;
+ * src/flucon2.f90:215-216).  A handle created with dgbgk_params.shard = 1
+ * and a vspace of its rings only (RORDER = the rings' count, VCORD their
+ * rows, SUMWEIGHT the full grid's; ALPHA = 1) is such a block.  Its step
+ * runs in phases on the handle's stream; between them the caller sums the
+ * exchange buffers over the shards (device memory the caller owns, of the
+ * sizes dgbgk_shard_sizes gives) -- an NCCL all-reduce enqueued on that
+ * stream, for one shard per GPU:
+ *   phase 1: pass-1 partial sums            -> sums1        (then SUM)
+ *   phase 2: pass-2 partial sums and walls  -> sums2        (then SUM)
+ *   phase 3: moments, MU, dt, ETA; the sweep of the shard's velocities;
+ *            the step's residual partials    -> res[2]      (then MAX of
+ *            res[0], SUM of res[1])
+ *   phase 4: the step's bookkeeping (histories, convergence test).
+ * dgbgk_shard_begin / _end bracket a run of steps as dgbgk_advance does
+ * (its max_steps, tol, histories and status); phases 0 (outside a run),
+ * 1, 2 and 5 give dgbgk_get_macros, _get_forces and _get_node_fields the
+ * moments of the current state.  dgbgk_advance, batches and the output ring
+ * refuse a shard. */
+int dgbgk_shard_stream(dgbgk_handle* h, void** stream);  /* the cudaStream_t of the phases */
+int dgbgk_shard_sizes(dgbgk_handle* h, long long* n_sums1, long long* n_sums2);  /* doubles */
+int dgbgk_shard_begin(dgbgk_handle* h, int max_steps, double tol);
+int dgbgk_shard_phase(dgbgk_handle* h, int phase, double* sums1, double* sums2, double* res);
+int dgbgk_shard_poll(dgbgk_handle* h, int* done);  /* synchronises the stream */
+int dgbgk_shard_end(dgbgk_handle* h, int* steps_done, double* res_linf, double* res_l2, double* dte, int* done);
 
 void dgbgk_destroy(dgbgk_handle* h);
 const char* dgbgk_last_error(void);

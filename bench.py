@@ -57,6 +57,9 @@ def args():
     ap.add_argument("--no-tc1", action="store_true", help="skip the reference test case tc1 leg")
     ap.add_argument("--no-large", action="store_true", help="skip the large-channel (400x200, 32x64) leg")
     ap.add_argument("--no-cavity", action="store_true", help="skip the cavity's time to residual 1e-8")
+    ap.add_argument("--shard", action="store_true",
+                    help="velocity-space shards: the workload's speed rings split over the ranks (strong scaling, "
+                         "NCCL all-reduces between the step's phases) instead of one replica per rank")
     return ap.parse_args()
 
 
@@ -465,6 +468,44 @@ def run_ours(a, d):
     return out
 
 
+def run_sharded(a, d):
+    """The workload split into whole speed rings over the ranks (one shard
+    per GPU, dgbgk.shard): a step is the library's four phases with three
+    all-reduces (NCCL, on the library's stream) between them; the time is
+    the max over the ranks of the device time of the timed steps."""
+    import torch
+    from dgbgk.shard import ShardedSolver, TorchGroup, advance_distributed, advance_local
+    torch.cuda.set_device(d.local)
+    case = make_case(a.config)
+    sh = ShardedSolver(case, d.rank, d.world, precision=a.precision, device=d.local)
+    sh.init_case()
+
+    def run(n):
+        if d.world > 1:
+            return advance_distributed(sh, n, group=TorchGroup(d.pg), poll_every=0)
+        return advance_local([sh], n, poll_every=0)[0]
+    run(max(a.warmup, 3))
+    clocks = Clocks(d.local)
+    d.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    r = run(a.steps)
+    torch.cuda.synchronize()
+    ck = clocks.stop()
+    d.barrier()
+    t_ms = d.max(sh.solver.last_ms())
+    assert r["steps"] == a.steps
+    rate = case.dofs * a.steps / (t_ms * 1e-3)  # the whole case advanced by all ranks together
+    sh.close()
+    return {"metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": d.world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": t_ms / a.steps, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f32" if a.precision == 32 else "f64",
+            "data": "synthetic (generated mesh and velocity grid; free-stream initial state)",
+            "config": dict(config_of(case, a.precision, 1),
+                           parallelism=f"velocity shards x{d.world} (whole speed rings per GPU)"),
+            "clocks": ck, "gpu_launches": a.steps * 7}
+
+
 def run_reference(a, d):
     if d.rank != 0:
         return None
@@ -486,7 +527,12 @@ def main():
     a = args()
     d = Dist()
     try:
-        out = run_reference(a, d) if a.impl == "reference" else run_ours(a, d)
+        if a.impl == "reference":
+            out = run_reference(a, d)
+        elif a.shard:
+            out = run_sharded(a, d)
+        else:
+            out = run_ours(a, d)
         if d.rank == 0 and out is not None:
             print(json.dumps(out), flush=True)
     finally:

@@ -120,7 +120,7 @@ _lib = None
 
 def use_library(path):
     """Loads the library from `path` (another build of the same ABI, e.g. a
-    compile-time variant) instead of lib/libdgbgk.so; call before the first
+    build kept for an A/B timing) instead of lib/libdgbgk.so; call before the first
     use."""
     global LIB_PATH
     if _lib is not None:

@@ -25,7 +25,7 @@ def main(argv=None):
     ap.add_argument("--tile-elems", type=int, default=0)
     ap.add_argument("--moment-rows", type=int, default=0, help="moment rows per warp step (1-4; 0: the library's)")
     ap.add_argument("--lib", default=None, help="a library build to time instead of lib/libdgbgk.so "
-                    "(e.g. a compile-time variant from `make variant`)")
+                    "(e.g. an earlier build kept for an A/B timing)")
     a = ap.parse_args(argv)
     if a.lib:
         from . import _lib

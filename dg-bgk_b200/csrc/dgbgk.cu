@@ -105,6 +105,7 @@ struct ImplBase {
   int mom_rows_req = 0;  // moment rows per warp step asked for at create (0: the heuristic)
   long long itime_total = 0;  // steps run since the state was last set (the reference's ITIME)
   bool shard = false;         // a velocity shard: its steps run through the shard phases
+  int srnd = 0;               // FP32: stochastic (dithered) rounding of the updated f
   // velocity-shard step phases (the caller sums the partials between them)
   virtual int shard_begin(int max_steps, double tol) = 0;
   virtual int shard_phase(int k, double* sums1, double* sums2, double* res) = 0;
@@ -618,6 +619,7 @@ template <class T> struct Impl : ImplBase {
     hc.nwall = (int)pl.walls.size();
     hc.rowbytes = (unsigned)(((size_t)pl.V * sizeof(T) + 15) / 16 * 16);
     hc.spec = pl.spec ? 1 : 0;
+    hc.srnd = srnd;
     hc.n_spec_par = (int)pl.spec_par.size();
     hc.n_spec_slots = (int)pl.welem.size();
     hc.rside = rside;
@@ -1389,6 +1391,11 @@ int dgbgk_create(const dgbgk_mesh* mesh, const dgbgk_vspace* vs, const dgbgk_par
   }
   impl->mom_rows_req = prm->moment_rows;
   impl->shard = prm->shard != 0;
+  if (prm->fp32_rounding != 0 && prm->fp32_rounding != 1) {
+    set_error("dgbgk_create: fp32_rounding must be 0 (to nearest) or 1 (stochastic)");
+    return DGBGK_EINVAL;
+  }
+  impl->srnd = prm->fp32_rounding;
   if (impl->shard && prm->alpha < 1.0) {
     set_error("dgbgk_create: a velocity shard needs ALPHA = 1 (the specular part reads mirrored velocities)");
     return DGBGK_EUNSUP;

@@ -152,6 +152,7 @@ template <class T> struct alignas(64) CaseDev {
   int nwall;          // FLUCON2 wall sides
   unsigned rowbytes;  // V*sizeof(T) rounded up to 16
   // ALPHA < 1: the specular part of the wall flux (the host plan's tables)
+  int srnd;                 // FP32: 1 = the new f is rounded stochastically (dithered), 0 = to nearest
   int spec;                 // 0: ALPHA = 1 or no wall side
   int n_spec_par, n_spec_slots;
   const int* rside;         // [B] reflection-table row, -1 off the walls
@@ -839,6 +840,35 @@ __device__ __forceinline__ void sweep_p1(const ElemRec<T>& r, const double* etab
   for (int i = 0; i < 3; ++i) vst<T>(tl + ro[i], f[i]);
 }
 
+// Stochastic rounding of the FP32 update f + d (no counterpart in the
+// reference; off unless the handle asks for it).  Round-to-nearest drops
+// every update below half an ulp, so an FP32 march stalls about
+// tau*ulp/2 from its fixed point along a mode that decays in tau steps;
+// adding a uniform dither in [-ulp/2, ulp/2) of f before the rounding
+// makes the stored value f + d in expectation (dithered rounding: Croci et
+// al., R. Soc. Open Sci. 9:211631, 2022), leaving zero-mean noise instead
+// of the stall.  The dither comes from a counter-based hash of the value's
+// index and the step (the same in a batch as alone, and from run to run).
+__device__ __forceinline__ unsigned srnd_hash(unsigned x, unsigned salt) {
+  unsigned h = x * 0x9E3779B1u + salt * 0x85EBCA77u;
+  h ^= h >> 15;
+  h *= 0x2C1B3C6Du;
+  h ^= h >> 12;
+  h *= 0x297A2D39u;
+  h ^= h >> 15;
+  return h;
+}
+// ulp of a normal FP32 value (0 below 2^-102, where no dither is added)
+__device__ __forceinline__ float ulp_f32(float f) {
+  const int ex = __float_as_int(f) & 0x7f800000;
+  return ex > (23 << 23) ? __int_as_float(ex - (23 << 23)) : 0.f;
+}
+// the dither of field k (10 bits) of h, times ulp(f): uniform in [-ulp/2, ulp/2)
+__device__ __forceinline__ float srnd_dither(unsigned h, int k, float f) {
+  const float u = (float)((h >> (10 * k)) & 1023u) * (1.f / 1024.f) + (0.5f / 1024.f - 0.5f);
+  return u * ulp_f32(f);
+}
+
 // max that keeps a NaN operand (max.NaN): the residual's "change the
 // unknown receives" must carry a non-finite update into the L2 sum
 __device__ __forceinline__ float fmax_nan(float a, float b) {
@@ -954,6 +984,7 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : (E
       const int cur = C.ctrl->cur;
       const double dtd = step_dt(C.ctrl);
       const T dt = (T)dtd, dth = (T)(0.5 * dtd), dth3 = (T)(0.5 * dtd / 3.0);
+      const unsigned salt = (unsigned)(C.ctrl->itime0 + C.ctrl->step);  // the step, for the FP32 dither
       double rmax = 0.0, rsq = 0.0;
 
       // unit prologue: block records and halo record heads (cp.async, one
@@ -1232,7 +1263,18 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : (E
                     ch = fmax_nan(d, -f);
                   else
                     ch = (f + d < (T)0) ? -f : d;
-                  T fn = fmax(f + d, (T)0);
+                  T fn;
+                  if constexpr (sizeof(T) == 4) {
+                    if (C.srnd) {  // dithered rounding of f + d (the value of DOF (e, i, vb + w) at this step)
+                      const unsigned hv =
+                          srnd_hash(((unsigned)(e0 + j) * 3u) * (unsigned)C.Vp + (unsigned)(vb + w), salt);
+                      fn = fmax(f + (d + srnd_dither(hv, i, f)), (T)0);
+                    } else {
+                      fn = fmax(f + d, (T)0);
+                    }
+                  } else {
+                    fn = fmax(f + d, (T)0);
+                  }
                   if (live) {
                     if (decltype(defer)::value && ((dmask >> (3 * w + i)) & 1u)) {
                       // deferred: k_wspec adds the specular part, clips and

@@ -48,6 +48,7 @@ class Params(ctypes.Structure):
         ("molar_mass", c_double), ("diameter", c_double), ("cinf", c_double * 4),
         ("precision", c_int), ("wall_velocity", POINTER(c_double)),
         ("tile_elems", c_int), ("moment_rows", c_int), ("device", c_int), ("shard", c_int),
+        ("fp32_rounding", c_int),
     ]
 
 

@@ -69,7 +69,7 @@ class Solver:
 
     def __init__(self, intma, coord, bsido, setup, vcord, sumweight, rorder, torder, rv, *, immat=1, csafm=0.5,
                  alpha=1.0, rgas=1.0, molar_mass=6.022e26, diameter=1.0, cinf=(0, 0, 0, 0), precision=64,
-                 wall_velocity=None, tile_elems=0, moment_rows=0, device=0, shard=0):
+                 wall_velocity=None, tile_elems=0, moment_rows=0, device=0, shard=0, fp32_rounding=0):
         L = lib()
         self._keep = []
 
@@ -114,13 +114,14 @@ class Solver:
         p.moment_rows = moment_rows
         p.device = device
         p.shard = shard
+        p.fp32_rounding = fp32_rounding
         h = c_void_p()
         check(L.dgbgk_create(ctypes.byref(m), ctypes.byref(vs), ctypes.byref(p), ctypes.byref(h)))
         self.h = h
         self.precision = precision
 
     @classmethod
-    def from_case(cls, case, precision=64, tile_elems=0, moment_rows=0, device=0):
+    def from_case(cls, case, precision=64, tile_elems=0, moment_rows=0, device=0, fp32_rounding=0):
         from .cases import gll
         m = case.mesh
         st = setup_mesh(m.intma, m.coord, m.bsido)
@@ -129,7 +130,7 @@ class Solver:
         s = cls(m.intma, m.coord, m.bsido, st, vc, sw, case.rorder, case.torder, case.rv, immat=case.immat,
                 csafm=case.csafm, alpha=case.alpha, rgas=case.rgas, molar_mass=case.molar_mass,
                 diameter=case.diameter, cinf=case.cinf, precision=precision, wall_velocity=m.wall_velocity,
-                tile_elems=tile_elems, moment_rows=moment_rows, device=device)
+                tile_elems=tile_elems, moment_rows=moment_rows, device=device, fp32_rounding=fp32_rounding)
         s.case = case
         s.setup = st
         s.vcord = vc

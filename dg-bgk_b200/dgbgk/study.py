@@ -332,7 +332,7 @@ def rel_fields(a, b):
             for i, k in enumerate(("n", "u", "v", "T"))}
 
 
-def evaluate(cases, ws, tol=1e-8, switch_tol=1e-5, max_steps=200000,
+def evaluate(cases, ws, tol=1e-8, switch_tol=1e-5, max_steps=200000, sr_switch_tol=1e-7,
              ways=("plain", "batch64", "batch64_warm", "fast"), log=None, device=0):
     """Time to tol for each way (see the module docstring); returns the
     results, the final normalised nodal fields per way and the cases kept."""
@@ -373,9 +373,9 @@ def evaluate(cases, ws, tol=1e-8, switch_tol=1e-5, max_steps=200000,
         if log:
             log(f"plain: {wall:.2f} s, steps {min(steps)}..{max(steps)}, dropped {out['dropped']}")
 
-    def batched(name, warm, precision_first, switch, rre=False):
+    def batched(name, warm, precision_first, switch, rre=False, srnd=0):
         t0 = time.perf_counter()
-        first = [Solver.from_case(c, precision=precision_first, device=device) for c in cases]
+        first = [Solver.from_case(c, precision=precision_first, device=device, fp32_rounding=srnd) for c in cases]
         fin = [Solver.from_case(c, precision=64, device=device) for c in cases] if switch else first
         t_setup = time.perf_counter() - t0
         t = time.perf_counter()
@@ -453,6 +453,14 @@ def evaluate(cases, ws, tol=1e-8, switch_tol=1e-5, max_steps=200000,
         out["fast_rre"] = batched("fast_rre", True, 32, switch_tol, rre=True)
     if "fast_cold_rre" in ways:
         out["fast_cold_rre"] = batched("fast_cold_rre", False, 32, switch_tol, rre=True)
+    # the FP32 phase with stochastically rounded stores: no rounding stall,
+    # so it runs on to sr_switch_tol (or its noise floor) before the handoff
+    if "fast_cold_sr_rre" in ways:
+        out["fast_cold_sr_rre"] = batched("fast_cold_sr_rre", False, 32, sr_switch_tol, rre=True, srnd=1)
+    if "fast_sr_rre" in ways:
+        out["fast_sr_rre"] = batched("fast_sr_rre", True, 32, sr_switch_tol, rre=True, srnd=1)
+    if "fast_cold_sr" in ways:
+        out["fast_cold_sr"] = batched("fast_cold_sr", False, 32, sr_switch_tol, srnd=1)
     if "plain" in final:
         for k in final:
             if k == "plain":

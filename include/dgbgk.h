@@ -92,6 +92,11 @@ typedef struct dgbgk_params {
                          passed has only its speed rings (RORDER = their
                          count), with the full grid's SUMWEIGHT -- and its
                          steps run through dgbgk_shard_* (0 = whole grid) */
+  int fp32_rounding;  /* FP32 f: how the updated value is stored -- 0 (default)
+                         rounded to nearest, as the reference's REAL build;
+                         1 stochastically (a uniform dither of +-ulp/2 from a
+                         hash of the value's index and the step), so updates
+                         below half an ulp still move the state on average */
 } dgbgk_params;
 
 /* Fills a dgbgk_params with the reference defaults of

@@ -52,7 +52,10 @@ def test_shards_equal_the_whole_grid(mk, world, prec):
     for k in ("rho", "u", "v", "temp", "ps"):
         assert rel_l2(a[k], b[k], 1.0 if k in "uv" else 0.0) <= tol, k
     if c.mesh.bsido[:, 3].tolist().count(4):
-        np.testing.assert_allclose(shards[0].solver.forces(), full.forces(), rtol=tol, atol=1e-13)
+        # lift is a small difference of pressure terms of drag's size: the
+        # tolerance is on the forces' scale
+        fb = np.array(full.forces())
+        np.testing.assert_allclose(shards[0].solver.forces(), fb, rtol=tol, atol=tol * np.abs(fb).max())
     for s in shards + [full]:
         s.close()
 

@@ -416,6 +416,9 @@ def run_ours(a, d):
                        "sides, Mach/Kn/obstacle drawn (dgbgk.study.draw_cases(8, 77))",
               "dofs_per_case": kept[0].dofs if kept else 0, "tol": 1e-8, "switch_tol": res["switch_tol"],
               "plain_fp64_s": res["plain"]["wall_s"], "plain_fp64_steps": int(sum(res["plain"]["steps"])),
+              "batch_shapes": res.get("batch_shapes"),
+              "timing": "wall seconds of each march from its initial state to tol (the plain arm one case after "
+                        "another); the batch shape is tuned once per precision beforehand, untimed",
               "warm_start": {"network": "3 -> 256 x 3 -> 32768 (n, u, v, T on 64 x 128), BF16 tcgen05 GEMMs, FP32 "
                                         "accumulation, Adam", "train_cases": len(keep),
                              "train_cases_drawn": "dgbgk.study.draw_cases(48, 78), FP32 batches to 1e-4",

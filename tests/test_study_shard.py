@@ -55,6 +55,7 @@ def _patch(study):
 
     study.Solver = _Fake
     study.Batch = lambda ss: _Fake()
+    study.tuned_batch = lambda ss: _Fake()
     study.march_batch = march
     study.nodal_fields = lambda s, c: float(c.info["mach"] * 10 + c.info["kn"])
     study.resampler = Res

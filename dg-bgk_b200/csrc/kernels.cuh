@@ -153,6 +153,7 @@ template <class T> struct alignas(64) CaseDev {
   unsigned rowbytes;  // V*sizeof(T) rounded up to 16
   // ALPHA < 1: the specular part of the wall flux (the host plan's tables)
   int srnd;                 // FP32: 1 = the new f is rounded stochastically (dithered), 0 = to nearest
+  const T* corr;            // FP32: a per-value correction added to every update (layout of f), or NULL
   int spec;                 // 0: ALPHA = 1 or no wall side
   int n_spec_par, n_spec_slots;
   const int* rside;         // [B] reflection-table row, -1 off the walls
@@ -1231,6 +1232,14 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : (E
                 }
               }
             }
+            // the FP64 defect correction of an FP32 march (dgbgk_set_correction)
+            VecT cr[3];
+            const bool hascorr = sizeof(T) == 4 && C.corr != nullptr;
+            if (hascorr) {
+#pragma unroll
+              for (int i = 0; i < 3; ++i)
+                cr[i] = *reinterpret_cast<const VecT*>(C.corr + ((size_t)(e0 + j) * 3 + i) * C.Vp + vb);
+            }
             // GETINC / CMMINC, ADTHEM (f >= 0), INFLOW; the padding past V
             // stays zero
             // defer: some node of this chunk waits for the specular part
@@ -1248,10 +1257,12 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : (E
                   T d, rr;
                   if (IMMAT == 1) {
                     d = mmdt[i] * rhs[i][w] + mudt[i] * qmf;
+                    if (hascorr) d += VO::get(cr[i], w);
                     rr = fabs(d);
                   } else {
                     const T x = rhs[i][w] * dt, cdt = mudt[i] * qmf;
                     d = r.mm[i] * x + cdt;
+                    if (hascorr) d += VO::get(cr[i], w);
                     rr = ((x >= (T)0) ? cmx[i] : cmn[i]) * x + cdt;
                     rr = rr > (T)0 ? rr : (T)0;
                   }
@@ -1822,6 +1833,17 @@ __global__ void k_from_internal(const T* __restrict__ src, S* __restrict__ dst, 
   S* d = dst + (size_t)eo * 3 * V;
   for (int i = 0; i < 3; ++i)
     for (int v = threadIdx.x; v < V; v += blockDim.x) d[(size_t)v * 3 + i] = (S)src[(en * 3 + i) * Vp + v];
+}
+
+// The defect correction of an FP32 march grows by the FP64 state after
+// one FP64 step minus the FP32 state after one (corrected) FP32 step from
+// the same state, both in the internal layout (same element order and
+// pitch): then the corrected FP32 step from that state reproduces the FP64
+// one, and the corrected iteration shares the FP64 iteration's fixed point.
+__global__ void k_correction(const double* __restrict__ f64, const float* __restrict__ f32, float* __restrict__ corr,
+                             size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    corr[i] = (float)((double)corr[i] + (f64[i] - (double)f32[i]));
 }
 
 // INICON2 (src/inicon2.f90:143-174) times an optional per-DG-node scale.

@@ -75,6 +75,8 @@ SIGNATURES = {
     "dgbgk_set_residual_reference": (c_int, [c_void_p, c_double]),
     "dgbgk_get_residual_reference": (c_int, [c_void_p, _PD]),
     "dgbgk_copy_state": (c_int, [c_void_p, c_void_p]),
+    "dgbgk_set_correction": (c_int, [c_void_p, c_void_p]),
+    "dgbgk_clear_correction": (c_int, [c_void_p]),
     "dgbgk_snapshot": (c_int, [c_void_p, c_int]),
     "dgbgk_extrapolate": (c_int, [c_void_p, c_int, _PD]),
     "dgbgk_get_macros": (c_int, [c_void_p, _PD, _PD, _PD, _PD, _PD, _PD]),

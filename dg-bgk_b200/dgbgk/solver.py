@@ -239,6 +239,14 @@ class Solver:
         device) and residual reference; same mesh and velocity grid."""
         check(lib().dgbgk_copy_state(self.h, other.h))
 
+    def add_correction_from(self, other64):
+        """(FP32 handle) c += other64's state - this state
+        (dgbgk_set_correction)."""
+        check(lib().dgbgk_set_correction(self.h, other64.h))
+
+    def clear_correction(self):
+        check(lib().dgbgk_clear_correction(self.h))
+
     # -- observables ----------------------------------------------------
     def macros(self):
         out = {k: np.zeros(self.NP) for k in ("nd", "rho", "u", "v", "ps", "temp")}

@@ -105,19 +105,13 @@ struct ImplBase {
   int mom_rows_req = 0;  // moment rows per warp step asked for at create (0: the heuristic)
   long long itime_total = 0;  // steps run since the state was last set (the reference's ITIME)
   bool shard = false;         // a velocity shard: its steps run through the shard phases
-  int srnd = 0;               // FP32: stochastic (dithered) rounding of the updated f
   // velocity-shard step phases (the caller sums the partials between them)
   virtual int shard_begin(int max_steps, double tol) = 0;
   virtual int shard_phase(int k, double* sums1, double* sums2, double* res) = 0;
   virtual int shard_end(int* steps, double* linf, double* l2, double* dt, int* done) = 0;
   virtual void* stream_ptr() = 0;
   virtual int shard_poll(int* done) = 0;
-  // the FP32 defect correction (FP32 handles only)
-  virtual int set_correction(ImplBase* from64) = 0;
-  virtual int clear_correction() = 0;
-  // the current state buffer in the internal layout (element order, pitch Vp)
-  virtual const void* state_ptr() const = 0;
-  int Vpitch = 0;
+
   // bumped when the case's device table entry changes (buffers moved,
   // re-blocked): a batch holding the case rebuilds its table
   unsigned gen = 0;
@@ -409,7 +403,6 @@ template <class T> struct Impl : ImplBase {
   double *d_gram = nullptr, *d_gamma = nullptr;
   CaseDev<T> hc;          // this case's table entry
   LaunchSet<T> single;    // this case alone
-  T* corr = nullptr;  // FP32: the defect correction added to every update (dgbgk_set_correction)
   // device observables: GETFOR's sides, the output ring and one direct record
   ForceSide* d_fs = nullptr;
   int out_every = 0, out_cap = 0;
@@ -465,7 +458,6 @@ template <class T> struct Impl : ImplBase {
     dfree(snaps);
     dfree(d_gram);
     dfree(d_gamma);
-    dfree(corr);
     dfree(d_fs);
     dfree(out_ring);
     dfree(out_count);
@@ -492,7 +484,6 @@ template <class T> struct Impl : ImplBase {
     CK(cudaEventCreate(&ev1));
     for (auto& e : evpoll) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     Vp = ((pl.V + 31) / 32) * 32;
-    Vpitch = Vp;
     const size_t n = (size_t)3 * pl.E * Vp;
     TRY(dalloc(&f[0], n));
     TRY(dalloc(&f[1], n));
@@ -628,8 +619,6 @@ template <class T> struct Impl : ImplBase {
     hc.nwall = (int)pl.walls.size();
     hc.rowbytes = (unsigned)(((size_t)pl.V * sizeof(T) + 15) / 16 * 16);
     hc.spec = pl.spec ? 1 : 0;
-    hc.srnd = srnd;
-    hc.corr = corr;
     hc.n_spec_par = (int)pl.spec_par.size();
     hc.n_spec_slots = (int)pl.welem.size();
     hc.rside = rside;
@@ -849,33 +838,6 @@ template <class T> struct Impl : ImplBase {
     return collect(hctrl[1], steps, linf, l2, dt);
   }
   void* stream_ptr() override { return (void*)st; }
-  const void* state_ptr() const override { return f[cur]; }
-  int set_correction(ImplBase* from64) override {
-    if constexpr (sizeof(T) != 4) {
-      set_error("dgbgk_set_correction: the corrected handle must store f in FP32");
-      return DGBGK_EINVAL;
-    } else {
-      CK(cudaSetDevice(device));
-      const size_t n = (size_t)3 * pl.E * Vp;
-      if (!corr) {
-        TRY(dalloc(&corr, n));
-        CK(cudaMemsetAsync(corr, 0, n * sizeof(T), st));
-        TRY(refresh());  // the case table now carries the correction
-      }
-      k_correction<<<(unsigned)std::min<size_t>((n + 255) / 256, (size_t)8 * nsm), 256, 0, st>>>(
-          (const double*)from64->state_ptr(), f[cur], corr, n);
-      CK(cudaGetLastError());
-      CK(cudaStreamSynchronize(st));
-      return 0;
-    }
-  }
-  int clear_correction() override {
-    if (!corr) return 0;
-    CK(cudaSetDevice(device));
-    CK(cudaStreamSynchronize(st));
-    dfree(corr);
-    return refresh();
-  }
   int shard_poll(int* done) override {
     CK(cudaMemcpyAsync(&hctrl[2], ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
@@ -1428,11 +1390,6 @@ int dgbgk_create(const dgbgk_mesh* mesh, const dgbgk_vspace* vs, const dgbgk_par
   }
   impl->mom_rows_req = prm->moment_rows;
   impl->shard = prm->shard != 0;
-  if (prm->fp32_rounding != 0 && prm->fp32_rounding != 1) {
-    set_error("dgbgk_create: fp32_rounding must be 0 (to nearest) or 1 (stochastic)");
-    return DGBGK_EINVAL;
-  }
-  impl->srnd = prm->fp32_rounding;
   if (impl->shard && prm->alpha < 1.0) {
     set_error("dgbgk_create: a velocity shard needs ALPHA = 1 (the specular part reads mirrored velocities)");
     return DGBGK_EUNSUP;
@@ -1516,22 +1473,6 @@ int dgbgk_snapshot(dgbgk_handle* h, int slot) {
 int dgbgk_extrapolate(dgbgk_handle* h, int n, double* gamma) {
   HCHECK(h);
   return h->impl->extrapolate(n, gamma);
-}
-int dgbgk_set_correction(dgbgk_handle* h32, dgbgk_handle* h64) {
-  HCHECK(h32);
-  HCHECK(h64);
-  ImplBase* a = h32->impl.get();
-  ImplBase* b = h64->impl.get();
-  if (a->prec != 32 || b->prec != 64)
-    return set_error("dgbgk_set_correction: an FP32 handle corrected from an FP64 handle"), DGBGK_EINVAL;
-  if (a->device != b->device || a->pl.E != b->pl.E || a->pl.V != b->pl.V || a->Vpitch != b->Vpitch ||
-      a->pl.perm != b->pl.perm)
-    return set_error("dgbgk_set_correction: the handles differ in device, mesh or velocity grid"), DGBGK_EINVAL;
-  return a->set_correction(b);
-}
-int dgbgk_clear_correction(dgbgk_handle* h) {
-  HCHECK(h);
-  return h->impl->clear_correction();
 }
 int dgbgk_copy_state(dgbgk_handle* dst, const dgbgk_handle* src) {
   HCHECK(dst);

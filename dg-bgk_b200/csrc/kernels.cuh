@@ -152,8 +152,6 @@ template <class T> struct alignas(64) CaseDev {
   int nwall;          // FLUCON2 wall sides
   unsigned rowbytes;  // V*sizeof(T) rounded up to 16
   // ALPHA < 1: the specular part of the wall flux (the host plan's tables)
-  int srnd;                 // FP32: 1 = the new f is rounded stochastically (dithered), 0 = to nearest
-  const T* corr;            // FP32: a per-value correction added to every update (layout of f), or NULL
   int spec;                 // 0: ALPHA = 1 or no wall side
   int n_spec_par, n_spec_slots;
   const int* rside;         // [B] reflection-table row, -1 off the walls
@@ -841,35 +839,6 @@ __device__ __forceinline__ void sweep_p1(const ElemRec<T>& r, const double* etab
   for (int i = 0; i < 3; ++i) vst<T>(tl + ro[i], f[i]);
 }
 
-// Stochastic rounding of the FP32 update f + d (no counterpart in the
-// reference; off unless the handle asks for it).  Round-to-nearest drops
-// every update below half an ulp, so an FP32 march stalls about
-// tau*ulp/2 from its fixed point along a mode that decays in tau steps;
-// adding a uniform dither in [-ulp/2, ulp/2) of f before the rounding
-// makes the stored value f + d in expectation (dithered rounding: Croci et
-// al., R. Soc. Open Sci. 9:211631, 2022), leaving zero-mean noise instead
-// of the stall.  The dither comes from a counter-based hash of the value's
-// index and the step (the same in a batch as alone, and from run to run).
-__device__ __forceinline__ unsigned srnd_hash(unsigned x, unsigned salt) {
-  unsigned h = x * 0x9E3779B1u + salt * 0x85EBCA77u;
-  h ^= h >> 15;
-  h *= 0x2C1B3C6Du;
-  h ^= h >> 12;
-  h *= 0x297A2D39u;
-  h ^= h >> 15;
-  return h;
-}
-// ulp of a normal FP32 value (0 below 2^-102, where no dither is added)
-__device__ __forceinline__ float ulp_f32(float f) {
-  const int ex = __float_as_int(f) & 0x7f800000;
-  return ex > (23 << 23) ? __int_as_float(ex - (23 << 23)) : 0.f;
-}
-// the dither of field k (10 bits) of h, times ulp(f): uniform in [-ulp/2, ulp/2)
-__device__ __forceinline__ float srnd_dither(unsigned h, int k, float f) {
-  const float u = (float)((h >> (10 * k)) & 1023u) * (1.f / 1024.f) + (0.5f / 1024.f - 0.5f);
-  return u * ulp_f32(f);
-}
-
 // max that keeps a NaN operand (max.NaN): the residual's "change the
 // unknown receives" must carry a non-finite update into the L2 sum
 __device__ __forceinline__ float fmax_nan(float a, float b) {
@@ -985,7 +954,6 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : (E
       const int cur = C.ctrl->cur;
       const double dtd = step_dt(C.ctrl);
       const T dt = (T)dtd, dth = (T)(0.5 * dtd), dth3 = (T)(0.5 * dtd / 3.0);
-      const unsigned salt = (unsigned)(C.ctrl->itime0 + C.ctrl->step);  // the step, for the FP32 dither
       double rmax = 0.0, rsq = 0.0;
 
       // unit prologue: block records and halo record heads (cp.async, one
@@ -1232,14 +1200,6 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : (E
                 }
               }
             }
-            // the FP64 defect correction of an FP32 march (dgbgk_set_correction)
-            VecT cr[3];
-            const bool hascorr = sizeof(T) == 4 && C.corr != nullptr;
-            if (hascorr) {
-#pragma unroll
-              for (int i = 0; i < 3; ++i)
-                cr[i] = *reinterpret_cast<const VecT*>(C.corr + ((size_t)(e0 + j) * 3 + i) * C.Vp + vb);
-            }
             // GETINC / CMMINC, ADTHEM (f >= 0), INFLOW; the padding past V
             // stays zero
             // defer: some node of this chunk waits for the specular part
@@ -1257,12 +1217,10 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : (E
                   T d, rr;
                   if (IMMAT == 1) {
                     d = mmdt[i] * rhs[i][w] + mudt[i] * qmf;
-                    if (hascorr) d += VO::get(cr[i], w);
                     rr = fabs(d);
                   } else {
                     const T x = rhs[i][w] * dt, cdt = mudt[i] * qmf;
                     d = r.mm[i] * x + cdt;
-                    if (hascorr) d += VO::get(cr[i], w);
                     rr = ((x >= (T)0) ? cmx[i] : cmn[i]) * x + cdt;
                     rr = rr > (T)0 ? rr : (T)0;
                   }
@@ -1274,18 +1232,7 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : (E
                     ch = fmax_nan(d, -f);
                   else
                     ch = (f + d < (T)0) ? -f : d;
-                  T fn;
-                  if constexpr (sizeof(T) == 4) {
-                    if (C.srnd) {  // dithered rounding of f + d (the value of DOF (e, i, vb + w) at this step)
-                      const unsigned hv =
-                          srnd_hash(((unsigned)(e0 + j) * 3u) * (unsigned)C.Vp + (unsigned)(vb + w), salt);
-                      fn = fmax(f + (d + srnd_dither(hv, i, f)), (T)0);
-                    } else {
-                      fn = fmax(f + d, (T)0);
-                    }
-                  } else {
-                    fn = fmax(f + d, (T)0);
-                  }
+                  T fn = fmax(f + d, (T)0);
                   if (live) {
                     if (decltype(defer)::value && ((dmask >> (3 * w + i)) & 1u)) {
                       // deferred: k_wspec adds the specular part, clips and
@@ -1833,17 +1780,6 @@ __global__ void k_from_internal(const T* __restrict__ src, S* __restrict__ dst, 
   S* d = dst + (size_t)eo * 3 * V;
   for (int i = 0; i < 3; ++i)
     for (int v = threadIdx.x; v < V; v += blockDim.x) d[(size_t)v * 3 + i] = (S)src[(en * 3 + i) * Vp + v];
-}
-
-// The defect correction of an FP32 march grows by the FP64 state after
-// one FP64 step minus the FP32 state after one (corrected) FP32 step from
-// the same state, both in the internal layout (same element order and
-// pitch): then the corrected FP32 step from that state reproduces the FP64
-// one, and the corrected iteration shares the FP64 iteration's fixed point.
-__global__ void k_correction(const double* __restrict__ f64, const float* __restrict__ f32, float* __restrict__ corr,
-                             size_t n) {
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-    corr[i] = (float)((double)corr[i] + (f64[i] - (double)f32[i]));
 }
 
 // INICON2 (src/inicon2.f90:143-174) times an optional per-DG-node scale.

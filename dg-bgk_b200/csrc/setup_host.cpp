@@ -32,7 +32,6 @@ extern "C" void dgbgk_default_params(dgbgk_params* p) {
   p->tile_elems = 0;
   p->moment_rows = 0;
   p->shard = 0;
-  p->fp32_rounding = 0;
   p->device = 0;
 }
 

@@ -48,7 +48,6 @@ class Params(ctypes.Structure):
         ("molar_mass", c_double), ("diameter", c_double), ("cinf", c_double * 4),
         ("precision", c_int), ("wall_velocity", POINTER(c_double)),
         ("tile_elems", c_int), ("moment_rows", c_int), ("device", c_int), ("shard", c_int),
-        ("fp32_rounding", c_int),
     ]
 
 
@@ -75,8 +74,6 @@ SIGNATURES = {
     "dgbgk_set_residual_reference": (c_int, [c_void_p, c_double]),
     "dgbgk_get_residual_reference": (c_int, [c_void_p, _PD]),
     "dgbgk_copy_state": (c_int, [c_void_p, c_void_p]),
-    "dgbgk_set_correction": (c_int, [c_void_p, c_void_p]),
-    "dgbgk_clear_correction": (c_int, [c_void_p]),
     "dgbgk_snapshot": (c_int, [c_void_p, c_int]),
     "dgbgk_extrapolate": (c_int, [c_void_p, c_int, _PD]),
     "dgbgk_get_macros": (c_int, [c_void_p, _PD, _PD, _PD, _PD, _PD, _PD]),

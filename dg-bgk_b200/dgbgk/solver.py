@@ -69,7 +69,7 @@ class Solver:
 
     def __init__(self, intma, coord, bsido, setup, vcord, sumweight, rorder, torder, rv, *, immat=1, csafm=0.5,
                  alpha=1.0, rgas=1.0, molar_mass=6.022e26, diameter=1.0, cinf=(0, 0, 0, 0), precision=64,
-                 wall_velocity=None, tile_elems=0, moment_rows=0, device=0, shard=0, fp32_rounding=0):
+                 wall_velocity=None, tile_elems=0, moment_rows=0, device=0, shard=0):
         L = lib()
         self._keep = []
 
@@ -114,14 +114,13 @@ class Solver:
         p.moment_rows = moment_rows
         p.device = device
         p.shard = shard
-        p.fp32_rounding = fp32_rounding
         h = c_void_p()
         check(L.dgbgk_create(ctypes.byref(m), ctypes.byref(vs), ctypes.byref(p), ctypes.byref(h)))
         self.h = h
         self.precision = precision
 
     @classmethod
-    def from_case(cls, case, precision=64, tile_elems=0, moment_rows=0, device=0, fp32_rounding=0):
+    def from_case(cls, case, precision=64, tile_elems=0, moment_rows=0, device=0):
         from .cases import gll
         m = case.mesh
         st = setup_mesh(m.intma, m.coord, m.bsido)
@@ -130,7 +129,7 @@ class Solver:
         s = cls(m.intma, m.coord, m.bsido, st, vc, sw, case.rorder, case.torder, case.rv, immat=case.immat,
                 csafm=case.csafm, alpha=case.alpha, rgas=case.rgas, molar_mass=case.molar_mass,
                 diameter=case.diameter, cinf=case.cinf, precision=precision, wall_velocity=m.wall_velocity,
-                tile_elems=tile_elems, moment_rows=moment_rows, device=device, fp32_rounding=fp32_rounding)
+                tile_elems=tile_elems, moment_rows=moment_rows, device=device)
         s.case = case
         s.setup = st
         s.vcord = vc
@@ -238,14 +237,6 @@ class Solver:
         """Takes `other`'s state (converted to this handle's precision on the
         device) and residual reference; same mesh and velocity grid."""
         check(lib().dgbgk_copy_state(self.h, other.h))
-
-    def add_correction_from(self, other64):
-        """(FP32 handle) c += other64's state - this state
-        (dgbgk_set_correction)."""
-        check(lib().dgbgk_set_correction(self.h, other64.h))
-
-    def clear_correction(self):
-        check(lib().dgbgk_clear_correction(self.h))
 
     # -- observables ----------------------------------------------------
     def macros(self):

@@ -264,66 +264,6 @@ def march_batch_rre(b, solvers, tol, max_steps, start=1e-2, every=100, m=8, stal
     return steps, rel.copy(), status, dev[0]
 
 
-def march_batch_refined(b32, s32, b64, s64, tol, max_steps, every=200, stall=0.8, floor_below=1e-5):
-    """FP32 steps (stochastically rounded stores) with an FP64 defect
-    correction, then an FP64 finish.  Every `every` steps each active case
-    takes one FP64 step and one corrected FP32 step from the same state;
-    their difference is added to the case's correction
-    (dgbgk_set_correction) and the FP64 result becomes its state, so the
-    corrected FP32 iteration converges to the FP64 fixed point instead of
-    the one FP32 arithmetic shifts.  A case's FP32 phase ends at tol, on
-    divergence, or when its corrected residual stops falling below
-    floor_below (the rounding noise); then every case finishes in FP64
-    from its corrected state.  Returns the FP32 and FP64 step counts, the
-    statuses and the device seconds."""
-    n = len(s32)
-    steps32 = np.zeros(n, dtype=np.int64)
-    steps64 = np.zeros(n, dtype=np.int64)
-    status = np.zeros(n, dtype=np.int32)
-    rel = np.full(n, np.inf)
-    prev = np.full(n, np.inf)
-    done = np.zeros(n, dtype=bool)
-    refs = np.array([s.residual_reference() for s in s32])
-    dev = 0.0
-    while not done.all() and steps32.max() < max_steps:
-        act = ~done
-        idx = np.flatnonzero(act)
-        for i in idx:
-            s64[i].copy_state_from(s32[i])
-        b64.set_active(act)
-        b64.advance(1, raise_on_error=False)
-        b32.set_active(act)
-        b32.advance(1, raise_on_error=False)
-        dev += (b64.last_ms() + b32.last_ms()) * 1e-3
-        for i in idx:
-            s32[i].add_correction_from(s64[i])
-            s32[i].copy_state_from(s64[i])
-        steps64[act] += 1
-        steps32[act] += 1
-        r = b32.advance(every, tol=tol, raise_on_error=False)
-        dev += b32.last_ms() * 1e-3
-        live = act & (status == 0)
-        steps32[live] += r["steps"][live]
-        status[live] = r["status"][live]
-        now = r["res_l2_last"] / np.maximum(refs, 1e-300)
-        rel = np.where(live & (r["steps"] > 0), now, rel)
-        ended = (rel <= tol * (1 + 1e-9)) | (status != 0) | ((rel > stall * prev) & (rel < floor_below))
-        prev = np.where(live, rel, prev)
-        done |= ended & act
-    b32.set_active(np.ones(n, dtype=bool))
-    b64.set_active(np.ones(n, dtype=bool))
-    ok = status == 0
-    for i in np.flatnonzero(ok):
-        s64[i].copy_state_from(s32[i])
-    b64.set_active(ok)
-    r2 = b64.advance(max_steps, tol=tol, raise_on_error=False)
-    dev += b64.last_ms() * 1e-3
-    b64.set_active(np.ones(n, dtype=bool))
-    steps64[ok] += r2["steps"][ok]
-    status[ok] = r2["status"][ok]
-    return steps32, steps64, status, dev
-
-
 def shard(n, rank, world):
     """The case indices one rank of `world` generates: rank, rank + world, ...
     (round robin, so every rank gets the same mix of mesh sizes and Mach
@@ -427,7 +367,7 @@ def rel_fields(a, b):
             for i, k in enumerate(("n", "u", "v", "T"))}
 
 
-def evaluate(cases, ws, tol=1e-8, switch_tol=1e-5, max_steps=200000, sr_switch_tol=1e-7,
+def evaluate(cases, ws, tol=1e-8, switch_tol=1e-5, max_steps=200000,
              ways=("plain", "batch64", "batch64_warm", "fast"), log=None, device=0):
     """Time to tol for each way (see the module docstring); returns the
     results, the final normalised nodal fields per way and the cases kept."""
@@ -473,9 +413,9 @@ def evaluate(cases, ws, tol=1e-8, switch_tol=1e-5, max_steps=200000, sr_switch_t
     if any(w != "plain" for w in ways):
         out["batch_shapes"] = {f"fp{p}": pretune(cases, p, device) for p in (32, 64)}
 
-    def batched(name, warm, precision_first, switch, rre=False, srnd=0):
+    def batched(name, warm, precision_first, switch, rre=False):
         t0 = time.perf_counter()
-        first = [Solver.from_case(c, precision=precision_first, device=device, fp32_rounding=srnd) for c in cases]
+        first = [Solver.from_case(c, precision=precision_first, device=device) for c in cases]
         fin = [Solver.from_case(c, precision=64, device=device) for c in cases] if switch else first
         t_setup = time.perf_counter() - t0
         t = time.perf_counter()
@@ -553,46 +493,6 @@ def evaluate(cases, ws, tol=1e-8, switch_tol=1e-5, max_steps=200000, sr_switch_t
         out["fast_rre"] = batched("fast_rre", True, 32, switch_tol, rre=True)
     if "fast_cold_rre" in ways:
         out["fast_cold_rre"] = batched("fast_cold_rre", False, 32, switch_tol, rre=True)
-    # the FP32 phase with stochastically rounded stores: no rounding stall,
-    # so it runs on to sr_switch_tol (or its noise floor) before the handoff
-    if "fast_cold_sr_rre" in ways:
-        out["fast_cold_sr_rre"] = batched("fast_cold_sr_rre", False, 32, sr_switch_tol, rre=True, srnd=1)
-    if "fast_sr_rre" in ways:
-        out["fast_sr_rre"] = batched("fast_sr_rre", True, 32, sr_switch_tol, rre=True, srnd=1)
-    if "fast_cold_sr" in ways:
-        out["fast_cold_sr"] = batched("fast_cold_sr", False, 32, sr_switch_tol, srnd=1)
-
-    def refined(name, warm):
-        """FP32 with the FP64 defect correction, then an FP64 finish."""
-        s32 = [Solver.from_case(c, precision=32, device=device, fp32_rounding=1) for c in cases]
-        s64 = [Solver.from_case(c, precision=64, device=device) for c in cases]
-        t = time.perf_counter()
-        if warm:
-            ws.warm(s32, cases)
-        else:
-            for s in s32:
-                s.init_case()
-        for s, ref in zip(s32, refs):
-            s.set_residual_reference(ref)
-        b32, b64 = tuned_batch(s32), tuned_batch(s64)
-        st32, st64, status, dev = march_batch_refined(b32, s32, b64, s64, tol, max_steps)
-        wall = time.perf_counter() - t
-        if (status != 0).any():
-            raise RuntimeError(f"{name}: a case diverged")
-        final[name] = [nodal_fields(s, c) for s, c in zip(s64, cases)]
-        b32.close()
-        b64.close()
-        for s in s32 + s64:
-            s.close()
-        if log:
-            log(f"{name}: {wall:.2f} s (device {dev:.2f} s), steps {int(st32.min())}..{int(st32.max())} "
-                f"+ fp64 {int(st64.min())}..{int(st64.max())}")
-        return {"wall_s": wall, "device_s": dev, "steps": [int(x) for x in st32],
-                "steps_fp64_finish": [int(x) for x in st64], "fell_back_to_cold": []}
-    if "fast_cold_ref" in ways:
-        out["fast_cold_ref"] = refined("fast_cold_ref", False)
-    if "fast_ref" in ways:
-        out["fast_ref"] = refined("fast_ref", True)
     if "plain" in final:
         for k in final:
             if k == "plain":

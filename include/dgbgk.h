@@ -92,11 +92,6 @@ typedef struct dgbgk_params {
                          passed has only its speed rings (RORDER = their
                          count), with the full grid's SUMWEIGHT -- and its
                          steps run through dgbgk_shard_* (0 = whole grid) */
-  int fp32_rounding;  /* FP32 f: how the updated value is stored -- 0 (default)
-                         rounded to nearest, as the reference's REAL build;
-                         1 stochastically (a uniform dither of +-ulp/2 from a
-                         hash of the value's index and the step), so updates
-                         below half an ulp still move the state on average */
 } dgbgk_params;
 
 /* Fills a dgbgk_params with the reference defaults of
@@ -165,18 +160,6 @@ int dgbgk_get_residual_reference(dgbgk_handle* h, double* res_l2_ref);
  * be on one device and built from the same mesh and velocity grid. */
 int dgbgk_copy_state(dgbgk_handle* dst, const dgbgk_handle* src);
 
-/* No counterpart in the reference: an FP32 march with an FP64 defect
- * correction (iterative refinement of the steady state).  The FP32
- * handle h32 keeps a per-value correction c (FP32, the layout of f, zero
- * at first) that every one of its steps adds to the update; this call
- * adds to c the FP64 handle's state minus h32's state.  Taken after one
- * FP64 step of h64 and one step of h32 from the same state (copied with
- * dgbgk_copy_state), it makes h32's next step from that state reproduce
- * the FP64 step, so the corrected FP32 iteration has the FP64 iteration's
- * fixed point rather than the one FP32 arithmetic shifts.  The handles
- * share device, mesh and velocity grid.  dgbgk_clear_correction drops c. */
-int dgbgk_set_correction(dgbgk_handle* h32, dgbgk_handle* h64);
-int dgbgk_clear_correction(dgbgk_handle* h);
 
 /* No counterpart in the reference.  Reduced-rank extrapolation of the
  * pseudo-time iterates, a way to reach the same fixed point in fewer steps:

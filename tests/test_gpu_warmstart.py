@@ -179,32 +179,3 @@ def test_extrapolated_march_reaches_the_same_fixed_point_sooner():
     plain.close()
     s.close()
 
-
-def test_defect_correction_reproduces_the_fp64_step():
-    # dgbgk_set_correction: after one FP64 step and one FP32 step from the
-    # same state, c = their difference; the corrected FP32 step from that
-    # state then lands on the FP64 step's result (to FP32 storage rounding),
-    # where the uncorrected FP32 step misses it by its arithmetic error
-    c = family_case(2.5, 0.07)
-    s32 = Solver.from_case(c, precision=32)
-    s32.init_case()
-    s32.advance(40)
-    f0 = s32.get_state(np.float32)
-    s64 = Solver.from_case(c, precision=64)
-    s64.copy_state_from(s32)
-    s64.advance(1)
-    g64 = s64.get_state()
-    s32.advance(1)
-    miss = rel_l2(s32.get_state(), g64)
-    s32.add_correction_from(s64)
-    s32.set_state(f0)
-    s32.advance(1)
-    hit = rel_l2(s32.get_state(), g64)
-    assert hit <= 1e-7 and hit < 0.3 * miss, (hit, miss)
-    # cleared, the handle steps as before
-    s32.clear_correction()
-    s32.set_state(f0)
-    s32.advance(1)
-    assert rel_l2(s32.get_state(), g64) == pytest.approx(miss, rel=1e-6)
-    s32.close()
-    s64.close()

@@ -192,6 +192,22 @@ inline int tiles_per_unit(long total_tiles, int grid0, int upc, int nvt) {
   return (nvt + ng - 1) / ng;
 }
 
+// The sweep's velocity-tile groups of a case (a work unit is one element
+// block at one group): nreg groups of t tiles, then the rest (t to 2t - 1
+// tiles) in groups of decreasing size (sweep_tail_tiles), so that the units
+// handed out last, whose length sets the launch's tail, are short.
+template <class T> void set_groups(CaseDev<T>& k, int nvt, int t) {
+  t = std::max(1, std::min(t, nvt));
+  k.tpu = t;
+  k.nreg = std::max(0, nvt / t - 1);
+  int r = nvt - k.nreg * t, m = 0;
+  while (r > 0) {
+    r -= sweep_tail_tiles(r);
+    ++m;
+  }
+  k.ngrp = k.nreg + m;
+}
+
 // Uploads the case table and picks the launch shapes.  Moments: per-warp
 // rings of R-row stages; picks (R, warps per CTA, ring stages) with the most
 // resident warps per SM (shared memory and registers), then the most rows in
@@ -250,7 +266,7 @@ int build_launch_set(LaunchSet<T>& L, const std::vector<CaseDev<T>>& cs, int eb,
   std::vector<int> off(3 * (size_t)(n + 1), 0);
   for (int c = 0; c < n; ++c) {
     const auto& k = cs[c];
-    const int units = k.nblocks * ((k.nvt + k.tpu - 1) / k.tpu);
+    const int units = k.nblocks * k.ngrp;
     const int groups = (3 * k.E + L.mom_rows - 1) / L.mom_rows;
     off[c + 1] = off[c] + units;
     off[(n + 1) + c + 1] = off[(n + 1) + c] + groups;
@@ -379,7 +395,7 @@ template <class T> struct Impl : ImplBase {
   T *cmax = nullptr, *cmin = nullptr;
   T* tabs = nullptr;  // moment tables [3][Vp]
   double *nraw = nullptr, *disux = nullptr, *disuy = nullptr, *disps = nullptr, *mu = nullptr;
-  T *cxT = nullptr, *cyT = nullptr, *nfT = nullptr;
+  T* swtab = nullptr;  // [NTAB][Vp] the sweep's velocity tables (cx, cy, NFINF, FP64: |c|^2)
   double *cxD = nullptr, *cyD = nullptr, *wjf = nullptr;
   T *bTw = nullptr, *bUw = nullptr, *bEta = nullptr;
   double* bEtaD = nullptr;
@@ -429,9 +445,7 @@ template <class T> struct Impl : ImplBase {
     dfree(disuy);
     dfree(disps);
     dfree(mu);
-    dfree(cxT);
-    dfree(cyT);
-    dfree(nfT);
+    dfree(swtab);
     dfree(cxD);
     dfree(cyD);
     dfree(wjf);
@@ -498,16 +512,16 @@ template <class T> struct Impl : ImplBase {
     TRY(dalloc(&disuy, ndg));
     TRY(dalloc(&disps, ndg));
     TRY(dalloc(&mu, ndg));
-    // sweep velocity tables, zero past V
-    std::vector<T> a(Vp, (T)0), b(Vp, (T)0), c(Vp, (T)0);
+    // sweep velocity tables, zero past V: cx, cy, NFINF and (FP64) |c|^2
+    // rounded once from the FP64 cx*cx + cy*cy
+    std::vector<T> sw(SweepGeo<T>::NTAB * (size_t)Vp, (T)0);
     for (int v = 0; v < pl.V; ++v) {
-      a[v] = (T)pl.cx[v];
-      b[v] = (T)pl.cy[v];
-      c[v] = (T)pl.nfinf[v];
+      sw[v] = (T)pl.cx[v];
+      sw[Vp + v] = (T)pl.cy[v];
+      sw[2 * (size_t)Vp + v] = (T)pl.nfinf[v];
+      if (SweepGeo<T>::NTAB == 4) sw[3 * (size_t)Vp + v] = (T)(pl.cx[v] * pl.cx[v] + pl.cy[v] * pl.cy[v]);
     }
-    TRY(upload(&cxT, a, st));
-    TRY(upload(&cyT, b, st));
-    TRY(upload(&nfT, c, st));
+    TRY(upload(&swtab, sw, st));
     TRY(upload(&cxD, pl.cx, st));
     TRY(upload(&cyD, pl.cy, st));
     TRY(upload(&wjf, pl.wjf, st));
@@ -583,9 +597,10 @@ template <class T> struct Impl : ImplBase {
     hc.rec = rec;
     hc.halo_off = halo_off;
     hc.halo_list = halo_list;
-    hc.cx = cxT;
-    hc.cy = cyT;
-    hc.nfinf = nfT;
+    hc.swtab = swtab;
+    hc.cx = swtab;
+    hc.cy = swtab + Vp;
+    hc.nfinf = swtab + 2 * (size_t)Vp;
     hc.tabs = tabs;
     hc.bTw = bTw;
     hc.bUw = bUw;
@@ -615,7 +630,7 @@ template <class T> struct Impl : ImplBase {
     hc.Vp = Vp;
     hc.nblocks = pl.nblocks;
     hc.nvt = nvt();
-    hc.tpu = tpu;
+    set_groups(hc, nvt(), tpu);
     hc.nwall = (int)pl.walls.size();
     hc.rowbytes = (unsigned)(((size_t)pl.V * sizeof(T) + 15) / 16 * 16);
     hc.spec = pl.spec ? 1 : 0;
@@ -1698,7 +1713,7 @@ template <class T> struct BatchImpl : BatchBase {
     }
     std::vector<CaseDev<T>> table;
     for (auto* c : cs) {
-      c->hc.tpu = tiles_per_unit(tiles, sps * nsm, u, c->nvt());
+      set_groups(c->hc, c->nvt(), tiles_per_unit(tiles, sps * nsm, u, c->nvt()));
       table.push_back(c->hc);
     }
     TRY(build_launch_set(L, table, e, immat, max_halo, nsm, st, rows));

@@ -123,7 +123,8 @@ template <class T> struct alignas(64) CaseDev {
   ElemRec<T>* rec;
   const int* halo_off;
   const int* halo_list;
-  const T* cx;     // [Vp] sweep tables, zero past V
+  const T* swtab;  // [NTAB][Vp] sweep tables cx, cy, NFINF (, |c|^2), zero past V
+  const T* cx;     // rows 0, 1, 2 of swtab
   const T* cy;
   const T* nfinf;
   const T* tabs;   // [3][Vp] cx, cy, WEIGHT*JAC*FRAC for the moments, zero past V
@@ -148,7 +149,8 @@ template <class T> struct alignas(64) CaseDev {
   Ctrl* ctrl;
   double MM, sigt;  // M/NA, PI*d*d
   T alpha, rgas;
-  int E, V, Vp, nblocks, nvt, tpu;
+  int E, V, Vp, nblocks, nvt;
+  int tpu, nreg, ngrp;  // velocity-tile groups of the sweep's units (sweep_group)
   int nwall;          // FLUCON2 wall sides
   unsigned rowbytes;  // V*sizeof(T) rounded up to 16
   // ALPHA < 1: the specular part of the wall flux (the host plan's tables)
@@ -163,6 +165,28 @@ template <class T> struct alignas(64) CaseDev {
   const int* spec_seq_off;  // [slots + 1]
   const int* spec_seq;
 };
+
+// Size of the next group of the sweep's tail when r tiles remain: half of
+// them, rounded up (two or one at the end).
+__host__ __device__ inline int sweep_tail_tiles(int r) { return r <= 2 ? r : (r + 1) / 2; }
+
+// Tiles [vt0, vt0 + ntl) of velocity-tile group g: groups below nreg hold
+// tpu tiles, the rest shrink (sweep_tail_tiles).
+template <class T> __device__ __forceinline__ void sweep_group(const CaseDev<T>& C, int g, int& vt0, int& ntl) {
+  if (g < C.nreg) {
+    vt0 = g * C.tpu;
+    ntl = C.tpu;
+    return;
+  }
+  int s = C.nreg * C.tpu, r = C.nvt - s;
+  for (int m = C.nreg; m < g; ++m) {
+    const int n = sweep_tail_tiles(r);
+    s += n;
+    r -= n;
+  }
+  vt0 = s;
+  ntl = sweep_tail_tiles(r);
+}
 
 template <class T> struct BatchArgs {
   const CaseDev<T>* cases;  // [ncases]
@@ -732,6 +756,8 @@ __device__ __forceinline__ void tma_store_2d(const CUtensorMap* map, int x, int 
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
 // the issuing thread's bulk stores have finished reading shared memory
 __device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+// ... all but the most recent one
+__device__ __forceinline__ void bulk_wait_read1() { asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory"); }
 // ... and their writes are complete
 __device__ __forceinline__ void bulk_wait0() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 
@@ -850,6 +876,19 @@ __device__ __forceinline__ double fmax_nan(double a, double b) {
   return (a != a || b != b) ? a + b : fmax(a, b);
 }
 
+// Adds the per-warp residual partials (max |d|, sum of squares) to a case's
+// accumulators.
+template <int NW>
+__device__ __forceinline__ void resid_add(Ctrl* ctrl, const double* red_m, const double* red_s) {
+  double mm = 0, ss = 0;
+  for (int w = 0; w < NW; ++w) {
+    mm = fmax(mm, red_m[w]);
+    ss += red_s[w];
+  }
+  atomicAdd(&ctrl->acc_sq, ss);
+  atomicMax(reinterpret_cast<unsigned long long*>(&ctrl->acc_max), (unsigned long long)__double_as_longlong(mm));
+}
+
 // Persistent sweep kernel: EB block elements, TPE*EB threads.  Work units are
 // (block b, group of `tpu` velocity tiles) with b fastest, handed out in
 // order (the first by blockIdx, the rest from a device counter), so the CTAs
@@ -933,6 +972,13 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : (E
   };
 
   int unit = blockIdx.x, c = 0, iter = 0;
+  // tiles this CTA has started: the two tile buffers are used in turn across
+  // units, so a unit's first tile goes to the buffer its predecessor's last
+  // tile did not use, whose box store was issued a tile earlier
+  int gk = 0;
+  // residual partials of the thread's values: a single case adds them to its
+  // control block once per CTA (after the last unit), a batch once per unit
+  double rmax = 0.0, rsq = 0.0;
   // the unit after this one, drawn ahead so the atomic's latency is hidden
   int next = (tid == 0 && unit < total_units) ? (int)gridDim.x + atomicAdd(&a.ctl->sweep_next, 1) : 0;
   while (unit < total_units) {
@@ -950,40 +996,61 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : (E
       const int b = lu % C.nblocks, vg = lu / C.nblocks;
       const int e0 = b * EB, nb = min(EB, C.E - e0);
       const int h0 = C.halo_off[b], nh = C.halo_off[b + 1] - h0;
-      const int vt0 = vg * C.tpu, ntl = min(C.tpu, C.nvt - vt0);
+      int vt0, ntl;
+      sweep_group(C, vg, vt0, ntl);
       const int cur = C.ctrl->cur;
       const double dtd = step_dt(C.ctrl);
       const T dt = (T)dtd, dth = (T)(0.5 * dtd), dth3 = (T)(0.5 * dtd / 3.0);
-      double rmax = 0.0, rsq = 0.0;
+      const int* __restrict__ hlist = C.halo_list + h0;
 
-      // unit prologue: block records and halo record heads (cp.async, one
-      // group), the halo's f rows and the velocity tables
+      // unit prologue, all of it asynchronous (the first tile's barrier
+      // publishes it): tile 0's block rows as TMA boxes (thread 0, once the
+      // buffer's last box store has read it) and its halo rows by cp.async,
+      // row numbers from the halo list; the block's element records, the
+      // halo's record heads and the unit's slices of the velocity tables
+      // (cp.async, in one group with the halo rows); the halo row list of
+      // the later tiles
       {
+        const int bi0 = gk & 1;
+        unsigned char* dst = base + (size_t)bi0 * tile_bytes;
+        if (tid == 0) {
+          bulk_wait_read1();  // the newest store reads the other buffer
+          fence_proxy_async_smem();
+          mbar_expect_tx(&bars[bi0], NBOX * BOX_BYTES);
+#pragma unroll
+          for (int x = 0; x < NBOX; ++x)
+            tma_load_2d(dst + x * BOX_BYTES, &C.tm[cur], vt0 * VT, 3 * e0 + x * G::BOX_ROWS, &bars[bi0]);
+        }
+        const T* srcf = C.f[cur] + (size_t)vt0 * VT;
+        for (int w = tid; w < nh * 12; w += NT) {
+          const int row = w >> 2, cq = w & 3, h = row / 3;
+          cp_async16(dst + (tile_row_off(3 * EB + row) ^ (16u * cq)),
+                     srcf + (size_t)(hlist[h] * 3 + (row - 3 * h)) * C.Vp + cq * W);
+        }
         const uint4* src = reinterpret_cast<const uint4*>(C.rec + e0);
         for (int w = tid; w < nb * RW; w += NT) cp_async16(reinterpret_cast<uint4*>(recs) + w, src + w);
-        const int* __restrict__ hlist = C.halo_list + h0;
         for (int w = tid; w < nh * HW; w += NT) {
           const int s = w / HW, k = w - s * HW;
           cp_async16(hrec + (size_t)s * HR + 16 * k, reinterpret_cast<const uint4*>(C.rec + hlist[s]) + k);
+        }
+        // table t's values [vt0*VT, (vt0 + ntl)*VT) to vtab + t*UV, 16 bytes a copy
+        constexpr int TW = VT * (int)sizeof(T) / 16;  // 16-byte words of one tile's values
+        const int nw = ntl * TW;
+        for (int w = tid; w < G::NTAB * nw; w += NT) {
+          const int t = w / nw, x = w - t * nw;
+          cp_async16(reinterpret_cast<uint4*>(vtab + t * UV) + x,
+                     reinterpret_cast<const uint4*>(C.swtab + (size_t)t * C.Vp + (size_t)vt0 * VT) + x);
         }
         cp_async_commit();
         for (int s = tid; s < 3 * nh; s += NT) {
           const int h = s / 3;
           hrow[s] = hlist[h] * 3 + (s - 3 * h);
         }
-        const int v0 = vt0 * VT;
-        for (int v = tid; v < ntl * VT; v += NT) {
-          const T cx = C.cx[v0 + v], cy = C.cy[v0 + v];
-          vtab[v] = cx;
-          vtab[UV + v] = cy;
-          vtab[2 * UV + v] = C.nfinf[v0 + v];
-          if (G::NTAB == 4) vtab[3 * UV + v] = cx * cx + cy * cy;
-        }
       }
-      // copies of tile vt into buffer bi: the block's rows (3*e0 ..) as NBOX
-      // TMA boxes issued by thread 0 once the buffer's last box store has
-      // read it (rows past 3E read as zeros), the halo rows (tile rows 3*EB
-      // ..) by cp.async, four threads per 64-byte row
+      // copies of tile vt (k >= 1) into buffer bi: the block's rows (3*e0 ..)
+      // as NBOX TMA boxes issued by thread 0 once the buffer's last box store
+      // has read it (rows past 3E read as zeros), the halo rows (tile rows
+      // 3*EB ..) by cp.async, four threads per 64-byte row
       auto issue = [&](int vt, int bi) {
         unsigned char* dst = base + (size_t)bi * tile_bytes;
         if (tid == 0) {
@@ -1000,13 +1067,10 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : (E
           cp_async16(dst + (tile_row_off(3 * EB + row) ^ (16u * cq)), src + (size_t)hrow[row] * C.Vp + cq * W);
         }
       };
-      __syncthreads();  // hrow, vtab
-      issue(vt0, 0);
-      cp_async_commit();
       const unsigned hx = 16u * CPT * hh;  // the thread's first chunk, as an offset XOR
 
-      for (int k = 0; k < ntl; ++k) {
-        const int bi = k & 1;
+      for (int k = 0; k < ntl; ++k, ++gk) {
+        const int bi = gk & 1;
         unsigned char* const tl = base + (size_t)bi * tile_bytes;
         // thread 0 waits for the boxes (the others wait in the barrier, not
         // spinning); every thread waits for its own halo copies
@@ -1292,38 +1356,47 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : (E
         }
         return;
       }
-      // the unit's residual, per warp
-      rmax = warp_max(rmax);
-      rsq = warp_sum(rsq);
-      if ((tid & 31) == 0) {
-        red_m[tid >> 5] = rmax;
-        red_s[tid >> 5] = rsq;
+      // a batch: the unit's residual, per warp
+      if (!ONE) {
+        rmax = warp_max(rmax);
+        rsq = warp_sum(rsq);
+        if ((tid & 31) == 0) {
+          red_m[tid >> 5] = rmax;
+          red_s[tid >> 5] = rsq;
+        }
+        rmax = rsq = 0.0;
       }
       last_map = &C.tm[cur ^ 1];
       last_vt = vt0 + ntl - 1;
-      last_bi = (ntl - 1) & 1;
+      last_bi = (gk - 1) & 1;
       last_y0 = 3 * e0;
     }
     // every thread is past phase 2 of the unit's last tile and has written
-    // its rows: store the last tile and add the unit's residual to its case
-    // (the sum of squares can differ in its last bits between runs: the
-    // order of the atomics varies); the records, tables and halo list may
-    // be replaced
+    // its rows: store the last tile and (a batch) add the unit's residual to
+    // its case (the sum of squares can differ in its last bits between runs:
+    // the order of the atomics varies); the records, tables and halo list
+    // may be replaced
     if (tid == 0) s_unit[iter & 1] = next;
     __syncthreads();
     if (tid == 0 && last_map) {
       store(last_map, last_vt, last_bi, last_y0);
-      double mm = 0, ss = 0;
-      for (int w = 0; w < NW; ++w) {
-        mm = fmax(mm, red_m[w]);
-        ss += red_s[w];
-      }
-      atomicAdd(&C.ctrl->acc_sq, ss);
-      atomicMax(reinterpret_cast<unsigned long long*>(&C.ctrl->acc_max), (unsigned long long)__double_as_longlong(mm));
+      if (!ONE) resid_add<NW>(C.ctrl, red_m, red_s);
     }
     unit = s_unit[iter & 1];
     ++iter;
     if (tid == 0 && unit < total_units) next = (int)gridDim.x + atomicAdd(&a.ctl->sweep_next, 1);
+  }
+  // a single case: the CTA's residual (only a CTA that updated values; the
+  // case's flag is the same for all of them)
+  if (ONE && gk > 0) {
+    rmax = warp_max(rmax);
+    rsq = warp_sum(rsq);
+    if ((tid & 31) == 0) {
+      red_m[tid >> 5] = rmax;
+      red_s[tid >> 5] = rsq;
+    }
+    __syncthreads();
+    if (tid == 0) resid_add<NW>(one.ctrl, red_m, red_s);
   }
   if (tid == 0) bulk_wait0();  // the last box stores are complete before the CTA exits
 }

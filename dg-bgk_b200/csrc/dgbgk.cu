@@ -227,13 +227,13 @@ int build_launch_set(LaunchSet<T>& L, const std::vector<CaseDev<T>>& cs, int eb,
   unsigned maxrow = 16;
   for (const auto& c : cs) maxrow = std::max(maxrow, c.rowbytes);
   // one case: its moment tables sit in shared memory
-  const size_t tbytes = one ? (3 * (size_t)cs[0].Vp * sizeof(T) + 127) / 128 * 128 : 0;
   const size_t cap = 227 * 1024;
   long best = -1;
   for (int R : {4, 3, 2, 1})
     for (int w : {20, 16, 12, 10, 8, 6, 5, 4, 3, 2, 1})
       for (int sg : {3, 2, 1}) {
         if (force_rows > 0 && R != force_rows) continue;
+        const size_t tbytes = one ? (mom_tables(R) * (size_t)cs[0].Vp * sizeof(T) + 127) / 128 * 128 : 0;
         if (w > 16 && !one) continue;  // 640 threads: the single-case kernel only
         const size_t bytes = 128 * (((size_t)w * sg * 8 + 127) / 128) + tbytes + (size_t)w * sg * R * maxrow;
         if (bytes > cap) continue;
@@ -393,7 +393,7 @@ template <class T> struct Impl : ImplBase {
   ElemRec<T>* rec = nullptr;
   int *halo_off = nullptr, *halo_list = nullptr;
   T *cmax = nullptr, *cmin = nullptr;
-  T* tabs = nullptr;  // moment tables [3][Vp]
+  T* tabs = nullptr;  // moment tables [MOM_TABS][Vp]
   double *nraw = nullptr, *disux = nullptr, *disuy = nullptr, *disps = nullptr, *mu = nullptr;
   T* swtab = nullptr;  // [NTAB][Vp] the sweep's velocity tables (cx, cy, NFINF, FP64: |c|^2)
   double *cxD = nullptr, *cyD = nullptr, *wjf = nullptr;
@@ -525,11 +525,13 @@ template <class T> struct Impl : ImplBase {
     TRY(upload(&cxD, pl.cx, st));
     TRY(upload(&cyD, pl.cy, st));
     TRY(upload(&wjf, pl.wjf, st));
-    std::vector<T> tb(3 * (size_t)Vp, (T)0);  // zero past V
+    std::vector<T> tb(MOM_TABS * (size_t)Vp, (T)0);  // zero past V; products rounded once from FP64
     for (int v = 0; v < pl.V; ++v) {
       tb[v] = (T)pl.cx[v];
       tb[Vp + v] = (T)pl.cy[v];
       tb[2 * (size_t)Vp + v] = (T)pl.wjf[v];
+      tb[3 * (size_t)Vp + v] = (T)(pl.wjf[v] * pl.cx[v]);
+      tb[4 * (size_t)Vp + v] = (T)(pl.wjf[v] * pl.cy[v]);
     }
     TRY(upload(&tabs, tb, st));
     std::vector<T> tw(pl.bTw.begin(), pl.bTw.end()), uw(pl.bUw.begin(), pl.bUw.end()),

@@ -127,7 +127,7 @@ template <class T> struct alignas(64) CaseDev {
   const T* cx;     // rows 0, 1, 2 of swtab
   const T* cy;
   const T* nfinf;
-  const T* tabs;   // [3][Vp] cx, cy, WEIGHT*JAC*FRAC for the moments, zero past V
+  const T* tabs;   // [MOM_TABS][Vp] moment tables: cx, cy, w = WEIGHT*JAC*FRAC, w*cx, w*cy; zero past V
   const T* bTw;    // per boundary side: wall temperature, wall velocity (x, y), ETA
   const T* bUw;
   T* bEta;
@@ -187,6 +187,11 @@ template <class T> __device__ __forceinline__ void sweep_group(const CaseDev<T>&
   vt0 = s;
   ntl = sweep_tail_tiles(r);
 }
+
+// Moment tables: the row modes read the first three, the element mode rows
+// 2 to 4 in its first pass and 0 to 2 in its second.
+constexpr int MOM_TABS = 5;
+__host__ __device__ constexpr int mom_tables(int R) { return R == 3 ? 5 : 3; }
 
 template <class T> struct BatchArgs {
   const CaseDev<T>* cases;  // [ncases]
@@ -324,21 +329,21 @@ template <> struct RowMath<float> {
 template <class T> struct ElemMath;
 
 template <> struct ElemMath<float> {
+  // pass 1 from the tables w, w*cx, w*cy (three FMAs per value)
   static __device__ __forceinline__ void pass1(const float* rows, unsigned pitch, const float* tb, int Vp, int nq,
                                                int lane, double (&s)[3][3]) {
-    const float4* cx = reinterpret_cast<const float4*>(tb);
-    const float4* cy = reinterpret_cast<const float4*>(tb + Vp);
     const float4* wj = reinterpret_cast<const float4*>(tb + 2 * Vp);
+    const float4* wx = reinterpret_cast<const float4*>(tb + 3 * Vp);
+    const float4* wy = reinterpret_cast<const float4*>(tb + 4 * Vp);
     float t[3][3] = {};
     for (int q = lane; q < nq; q += 32) {
-      const float4 c = cx[q], d = cy[q], w = wj[q];
+      const float4 w = wj[q], c = wx[q], d = wy[q];
 #pragma unroll
       for (int r = 0; r < 3; ++r) {
         const float4 x = reinterpret_cast<const float4*>(reinterpret_cast<const unsigned char*>(rows) + r * pitch)[q];
-        const float a0 = w.x * x.x, a1 = w.y * x.y, a2 = w.z * x.z, a3 = w.w * x.w;
-        t[r][0] += (a0 + a1) + (a2 + a3);
-        t[r][1] = fmaf(c.x, a0, fmaf(c.y, a1, fmaf(c.z, a2, fmaf(c.w, a3, t[r][1]))));
-        t[r][2] = fmaf(d.x, a0, fmaf(d.y, a1, fmaf(d.z, a2, fmaf(d.w, a3, t[r][2]))));
+        t[r][0] = fmaf(w.x, x.x, fmaf(w.y, x.y, fmaf(w.z, x.z, fmaf(w.w, x.w, t[r][0]))));
+        t[r][1] = fmaf(c.x, x.x, fmaf(c.y, x.y, fmaf(c.z, x.z, fmaf(c.w, x.w, t[r][1]))));
+        t[r][2] = fmaf(d.x, x.x, fmaf(d.y, x.y, fmaf(d.z, x.z, fmaf(d.w, x.w, t[r][2]))));
       }
     }
 #pragma unroll
@@ -381,22 +386,22 @@ template <> struct ElemMath<float> {
 };
 
 template <> struct ElemMath<double> {
+  // pass 1 from the tables w, w*cx, w*cy (three FMAs per value)
   static __device__ __forceinline__ void pass1(const double* rows, unsigned pitch, const double* tb, int Vp, int nq,
                                                int lane, double (&s)[3][3]) {
-    const double2* cx = reinterpret_cast<const double2*>(tb);
-    const double2* cy = reinterpret_cast<const double2*>(tb + Vp);
     const double2* wj = reinterpret_cast<const double2*>(tb + 2 * Vp);
+    const double2* wx = reinterpret_cast<const double2*>(tb + 3 * Vp);
+    const double2* wy = reinterpret_cast<const double2*>(tb + 4 * Vp);
 #pragma unroll
     for (int r = 0; r < 3; ++r) s[r][0] = s[r][1] = s[r][2] = 0.0;
     for (int q = lane; q < nq; q += 32) {
-      const double2 c = cx[q], d = cy[q], w = wj[q];
+      const double2 w = wj[q], c = wx[q], d = wy[q];
 #pragma unroll
       for (int r = 0; r < 3; ++r) {
         const double2 x = reinterpret_cast<const double2*>(reinterpret_cast<const unsigned char*>(rows) + r * pitch)[q];
-        const double a0 = w.x * x.x, a1 = w.y * x.y;
-        s[r][0] += a0 + a1;
-        s[r][1] = fma(c.x, a0, fma(c.y, a1, s[r][1]));
-        s[r][2] = fma(d.x, a0, fma(d.y, a1, s[r][2]));
+        s[r][0] = fma(w.x, x.x, fma(w.y, x.y, s[r][0]));
+        s[r][1] = fma(c.x, x.x, fma(c.y, x.y, s[r][1]));
+        s[r][2] = fma(d.x, x.x, fma(d.y, x.y, s[r][2]));
       }
     }
   }
@@ -499,11 +504,12 @@ __global__ void __launch_bounds__(ONE ? 640 : 512, 1)
   // layout: [barriers][tables [3][Vp] (ONE)][rings: warp, stage, R rows]
   uint64_t* bars = reinterpret_cast<uint64_t*>(sm_raw) + warp * nstage;
   T* tb1 = reinterpret_cast<T*>(sm_raw + 128 * (((size_t)nwarp * nstage * 8 + 127) / 128));
-  const size_t tbytes = ONE ? (3 * (size_t)one.Vp * sizeof(T) + 127) / 128 * 128 : 0;
+  constexpr int NTB = mom_tables(R);  // tables staged for a single case
+  const size_t tbytes = ONE ? (NTB * (size_t)one.Vp * sizeof(T) + 127) / 128 * 128 : 0;
   const size_t stage_bytes = (size_t)R * a.mom_rowbytes;
   unsigned char* ring = reinterpret_cast<unsigned char*>(tb1) + tbytes + (size_t)warp * nstage * stage_bytes;
   if (ONE)
-    for (int i = threadIdx.x; i < 3 * one.Vp; i += blockDim.x) tb1[i] = one.tabs[i];
+    for (int i = threadIdx.x; i < NTB * one.Vp; i += blockDim.x) tb1[i] = one.tabs[i];
   const int gw = blockIdx.x * nwarp + warp, stride = gridDim.x * nwarp;
   if (lane == 0) {
     for (int s = 0; s < nstage; ++s) mbar_init(&bars[s], 1);
@@ -574,8 +580,9 @@ __global__ void __launch_bounds__(ONE ? 640 : 512, 1)
         for (int k = 0; k < 3; ++k) m1[r][k] = group_sum<32>(m1[r][k]);
         u[r][0] = u[r][1] = 0.0;
         if (m1[r][0] >= TINY_D) {  // src/macros.f90:126-134
-          u[r][0] = m1[r][1] / m1[r][0];
-          u[r][1] = m1[r][2] / m1[r][0];
+          const double inv = 1.0 / m1[r][0];
+          u[r][0] = m1[r][1] * inv;
+          u[r][1] = m1[r][2] * inv;
         }
       }
       ElemMath<T>::pass2(rows, C.rowbytes, tb, C.Vp, nql, lane, u, m2);
@@ -606,8 +613,9 @@ __global__ void __launch_bounds__(ONE ? 640 : 512, 1)
       nd = ux = uy = 0;
       if (s0 >= TINY_D) {  // src/macros.f90:126-134
         nd = s0;
-        ux = s1 / s0;
-        uy = s2 / s0;
+        const double inv = 1.0 / s0;
+        ux = s1 * inv;
+        uy = s2 * inv;
       }
       sp = sc = 0;
       RowMath<T>::pass2(row, tb, C.Vp, nqr, sub, L, ux, uy, sp, sc);

@@ -193,12 +193,21 @@ inline int tiles_per_unit(long total_tiles, int grid0, int upc, int nvt) {
 }
 
 // The sweep's velocity-tile groups of a case (a work unit is one element
-// block at one group): nreg groups of t tiles, then the rest (t to 2t - 1
-// tiles) in groups of decreasing size (sweep_tail_tiles), so that the units
-// handed out last, whose length sets the launch's tail, are short.
-template <class T> void set_groups(CaseDev<T>& k, int nvt, int t) {
+// block at one group): groups of t tiles and the rest.  A single case
+// (halve) ends with t to 2t - 1 tiles in groups of decreasing size
+// (sweep_tail_tiles), so that the units handed out last, which set the
+// launch's tail, are short; in a batch only the last case's units end the
+// launch, and the extra units would cost more than they save (measured on
+// eight 100x100 channels: FP64 batch step +6%).
+template <class T> void set_groups(CaseDev<T>& k, int nvt, int t, bool halve) {
   t = std::max(1, std::min(t, nvt));
   k.tpu = t;
+  k.halve = halve ? 1 : 0;
+  if (!halve) {
+    k.nreg = (nvt - 1) / t;
+    k.ngrp = k.nreg + 1;
+    return;
+  }
   k.nreg = std::max(0, nvt / t - 1);
   int r = nvt - k.nreg * t, m = 0;
   while (r > 0) {
@@ -632,7 +641,7 @@ template <class T> struct Impl : ImplBase {
     hc.Vp = Vp;
     hc.nblocks = pl.nblocks;
     hc.nvt = nvt();
-    set_groups(hc, nvt(), tpu);
+    set_groups(hc, nvt(), tpu, true);
     hc.nwall = (int)pl.walls.size();
     hc.rowbytes = (unsigned)(((size_t)pl.V * sizeof(T) + 15) / 16 * 16);
     hc.spec = pl.spec ? 1 : 0;
@@ -1715,7 +1724,7 @@ template <class T> struct BatchImpl : BatchBase {
     }
     std::vector<CaseDev<T>> table;
     for (auto* c : cs) {
-      set_groups(c->hc, c->nvt(), tiles_per_unit(tiles, sps * nsm, u, c->nvt()));
+      set_groups(c->hc, c->nvt(), tiles_per_unit(tiles, sps * nsm, u, c->nvt()), cs.size() == 1);
       table.push_back(c->hc);
     }
     TRY(build_launch_set(L, table, e, immat, max_halo, nsm, st, rows));

@@ -150,7 +150,7 @@ template <class T> struct alignas(64) CaseDev {
   double MM, sigt;  // M/NA, PI*d*d
   T alpha, rgas;
   int E, V, Vp, nblocks, nvt;
-  int tpu, nreg, ngrp;  // velocity-tile groups of the sweep's units (sweep_group)
+  int tpu, nreg, ngrp, halve;  // velocity-tile groups of the sweep's units (sweep_group)
   int nwall;          // FLUCON2 wall sides
   unsigned rowbytes;  // V*sizeof(T) rounded up to 16
   // ALPHA < 1: the specular part of the wall flux (the host plan's tables)
@@ -171,7 +171,8 @@ template <class T> struct alignas(64) CaseDev {
 __host__ __device__ inline int sweep_tail_tiles(int r) { return r <= 2 ? r : (r + 1) / 2; }
 
 // Tiles [vt0, vt0 + ntl) of velocity-tile group g: groups below nreg hold
-// tpu tiles, the rest shrink (sweep_tail_tiles).
+// tpu tiles, the rest is one group or (halve) shrinking groups
+// (sweep_tail_tiles).
 template <class T> __device__ __forceinline__ void sweep_group(const CaseDev<T>& C, int g, int& vt0, int& ntl) {
   if (g < C.nreg) {
     vt0 = g * C.tpu;
@@ -179,6 +180,11 @@ template <class T> __device__ __forceinline__ void sweep_group(const CaseDev<T>&
     return;
   }
   int s = C.nreg * C.tpu, r = C.nvt - s;
+  if (!C.halve) {
+    vt0 = s;
+    ntl = r;
+    return;
+  }
   for (int m = C.nreg; m < g; ++m) {
     const int n = sweep_tail_tiles(r);
     s += n;
@@ -188,8 +194,9 @@ template <class T> __device__ __forceinline__ void sweep_group(const CaseDev<T>&
   ntl = sweep_tail_tiles(r);
 }
 
-// Moment tables: the row modes read the first three, the element mode rows
-// 2 to 4 in its first pass and 0 to 2 in its second.
+// Moment tables: the row modes read the first three; the element mode of a
+// single case (tables in shared memory) rows 2 to 4 in its first pass and 0
+// to 2 in its second, of a batch (tables through L1) the first three.
 constexpr int MOM_TABS = 5;
 __host__ __device__ constexpr int mom_tables(int R) { return R == 3 ? 5 : 3; }
 
@@ -329,21 +336,31 @@ template <> struct RowMath<float> {
 template <class T> struct ElemMath;
 
 template <> struct ElemMath<float> {
-  // pass 1 from the tables w, w*cx, w*cy (three FMAs per value)
+  // pass 1.  TAB: from the tables w, w*cx, w*cy (three FMAs per value;
+  // tables in shared memory); otherwise from w, cx, cy (w*f, then three
+  // sums; the tables the second pass reads too, through L1)
+  template <bool TAB>
   static __device__ __forceinline__ void pass1(const float* rows, unsigned pitch, const float* tb, int Vp, int nq,
                                                int lane, double (&s)[3][3]) {
     const float4* wj = reinterpret_cast<const float4*>(tb + 2 * Vp);
-    const float4* wx = reinterpret_cast<const float4*>(tb + 3 * Vp);
-    const float4* wy = reinterpret_cast<const float4*>(tb + 4 * Vp);
+    const float4* wx = reinterpret_cast<const float4*>(tb + (TAB ? 3 : 0) * Vp);
+    const float4* wy = reinterpret_cast<const float4*>(tb + (TAB ? 4 : 1) * Vp);
     float t[3][3] = {};
     for (int q = lane; q < nq; q += 32) {
       const float4 w = wj[q], c = wx[q], d = wy[q];
 #pragma unroll
       for (int r = 0; r < 3; ++r) {
         const float4 x = reinterpret_cast<const float4*>(reinterpret_cast<const unsigned char*>(rows) + r * pitch)[q];
-        t[r][0] = fmaf(w.x, x.x, fmaf(w.y, x.y, fmaf(w.z, x.z, fmaf(w.w, x.w, t[r][0]))));
-        t[r][1] = fmaf(c.x, x.x, fmaf(c.y, x.y, fmaf(c.z, x.z, fmaf(c.w, x.w, t[r][1]))));
-        t[r][2] = fmaf(d.x, x.x, fmaf(d.y, x.y, fmaf(d.z, x.z, fmaf(d.w, x.w, t[r][2]))));
+        if constexpr (TAB) {
+          t[r][0] = fmaf(w.x, x.x, fmaf(w.y, x.y, fmaf(w.z, x.z, fmaf(w.w, x.w, t[r][0]))));
+          t[r][1] = fmaf(c.x, x.x, fmaf(c.y, x.y, fmaf(c.z, x.z, fmaf(c.w, x.w, t[r][1]))));
+          t[r][2] = fmaf(d.x, x.x, fmaf(d.y, x.y, fmaf(d.z, x.z, fmaf(d.w, x.w, t[r][2]))));
+        } else {
+          const float a0 = w.x * x.x, a1 = w.y * x.y, a2 = w.z * x.z, a3 = w.w * x.w;
+          t[r][0] += (a0 + a1) + (a2 + a3);
+          t[r][1] = fmaf(c.x, a0, fmaf(c.y, a1, fmaf(c.z, a2, fmaf(c.w, a3, t[r][1]))));
+          t[r][2] = fmaf(d.x, a0, fmaf(d.y, a1, fmaf(d.z, a2, fmaf(d.w, a3, t[r][2]))));
+        }
       }
     }
 #pragma unroll
@@ -386,12 +403,13 @@ template <> struct ElemMath<float> {
 };
 
 template <> struct ElemMath<double> {
-  // pass 1 from the tables w, w*cx, w*cy (three FMAs per value)
+  // pass 1, TAB as for FP32
+  template <bool TAB>
   static __device__ __forceinline__ void pass1(const double* rows, unsigned pitch, const double* tb, int Vp, int nq,
                                                int lane, double (&s)[3][3]) {
     const double2* wj = reinterpret_cast<const double2*>(tb + 2 * Vp);
-    const double2* wx = reinterpret_cast<const double2*>(tb + 3 * Vp);
-    const double2* wy = reinterpret_cast<const double2*>(tb + 4 * Vp);
+    const double2* wx = reinterpret_cast<const double2*>(tb + (TAB ? 3 : 0) * Vp);
+    const double2* wy = reinterpret_cast<const double2*>(tb + (TAB ? 4 : 1) * Vp);
 #pragma unroll
     for (int r = 0; r < 3; ++r) s[r][0] = s[r][1] = s[r][2] = 0.0;
     for (int q = lane; q < nq; q += 32) {
@@ -399,9 +417,16 @@ template <> struct ElemMath<double> {
 #pragma unroll
       for (int r = 0; r < 3; ++r) {
         const double2 x = reinterpret_cast<const double2*>(reinterpret_cast<const unsigned char*>(rows) + r * pitch)[q];
-        s[r][0] = fma(w.x, x.x, fma(w.y, x.y, s[r][0]));
-        s[r][1] = fma(c.x, x.x, fma(c.y, x.y, s[r][1]));
-        s[r][2] = fma(d.x, x.x, fma(d.y, x.y, s[r][2]));
+        if constexpr (TAB) {
+          s[r][0] = fma(w.x, x.x, fma(w.y, x.y, s[r][0]));
+          s[r][1] = fma(c.x, x.x, fma(c.y, x.y, s[r][1]));
+          s[r][2] = fma(d.x, x.x, fma(d.y, x.y, s[r][2]));
+        } else {
+          const double a0 = w.x * x.x, a1 = w.y * x.y;
+          s[r][0] += a0 + a1;
+          s[r][1] = fma(c.x, a0, fma(c.y, a1, s[r][1]));
+          s[r][2] = fma(d.x, a0, fma(d.y, a1, s[r][2]));
+        }
       }
     }
   }
@@ -573,7 +598,7 @@ __global__ void __launch_bounds__(ONE ? 640 : 512, 1)
     if constexpr (ELEM) {
       const T* rows = reinterpret_cast<const T*>(ring + (size_t)s * stage_bytes);
       double m1[3][3], u[3][2], m2[3][2];
-      ElemMath<T>::pass1(rows, C.rowbytes, tb, C.Vp, nql, lane, m1);
+      ElemMath<T>::template pass1<ONE>(rows, C.rowbytes, tb, C.Vp, nql, lane, m1);
 #pragma unroll
       for (int r = 0; r < 3; ++r) {
 #pragma unroll

@@ -561,7 +561,10 @@ template <class T> struct Impl : ImplBase {
       TRY(upload(&rf_i, pl.rf_i, st));
       TRY(upload(&rf_z, rz, st));
       TRY(upload(&welem, pl.welem, st));
-      TRY(dalloc(&wd, std::max<size_t>(1, pl.welem.size() * 3 * (size_t)Vp)));
+      // deferred wall values: IMMAT = 1 DELUN without the specular part;
+      // IMMAT = 0 RHS*DTE and COLL*DTE (two halves), whose CMMINC residual
+      // needs them apart
+      TRY(dalloc(&wd, std::max<size_t>(1, (pl.immat == 0 ? 2 : 1) * pl.welem.size() * 3 * (size_t)Vp)));
       std::vector<int> one1(1, 0);
       TRY(upload(&spec_par, pl.spec_par.empty() ? one1 : pl.spec_par, st));
       TRY(upload(&spec_seq_off, pl.spec_seq_off, st));
@@ -645,6 +648,7 @@ template <class T> struct Impl : ImplBase {
     hc.nwall = (int)pl.walls.size();
     hc.rowbytes = (unsigned)(((size_t)pl.V * sizeof(T) + 15) / 16 * 16);
     hc.spec = pl.spec ? 1 : 0;
+    hc.immat = pl.immat;
     hc.n_spec_par = (int)pl.spec_par.size();
     hc.n_spec_slots = (int)pl.welem.size();
     hc.rside = rside;
@@ -1104,8 +1108,10 @@ template <class T> struct Impl : ImplBase {
       snaps = nb;
       snap_cap = slot + 1;
     }
+    // on the case's stream, not waited for: every later use of the state or
+    // the snapshots (a step, a batch advance, dgbgk_extrapolate, a copy out)
+    // is ordered behind it on that stream or waits for it
     CK(cudaMemcpyAsync(snaps + (size_t)slot * N, f[cur], N * sizeof(T), cudaMemcpyDeviceToDevice, st));
-    CK(cudaStreamSynchronize(st));
     return 0;
   }
   int extrapolate(int n, double* gamma) override {
@@ -1166,9 +1172,11 @@ template <class T> struct Impl : ImplBase {
       }
     if (gamma) std::copy(g.begin(), g.end(), gamma);
     CK(cudaMemcpyAsync(d_gamma, g.data(), m * sizeof(double), cudaMemcpyHostToDevice, st));
+    // gamma is staged by the copy before it returns (pageable source); the
+    // new state is written on the case's stream, which every later use of
+    // it follows or waits for
     k_combine<T><<<grid, 256, 0, st>>>(snaps, N, m, d_gamma, N, f[cur]);
     CK(cudaGetLastError());
-    CK(cudaStreamSynchronize(st));
     ++epoch;
     return 0;
   }
@@ -1646,6 +1654,7 @@ template <class T> struct BatchImpl : BatchBase {
   cudaGraphExec_t gexec = nullptr;
   int* d_done = nullptr;
   int* h_done = nullptr;  // pinned [2]
+  double* h_l2 = nullptr;  // pinned [ncases]: the cases' last L2 residuals
   int rows = 0;           // moment rows per warp step (0: the heuristic)
   // ms per step: (eb 64, 128) x (upc 2, 4, 8, 16), then moment rows 1, 2, 3, 4;
   // 0 = not tried
@@ -1664,6 +1673,7 @@ template <class T> struct BatchImpl : BatchBase {
     L.release();
     dfree(d_done);
     if (h_done) cudaFreeHost(h_done);
+    if (h_l2) cudaFreeHost(h_l2);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     for (auto& e : evp)
@@ -1689,6 +1699,7 @@ template <class T> struct BatchImpl : BatchBase {
     for (auto& e : evp) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     TRY(dalloc(&d_done, 1));
     CK(cudaMallocHost((void**)&h_done, 2 * sizeof(int)));
+    CK(cudaMallocHost((void**)&h_l2, cs.size() * sizeof(double)));
     tune_ms.assign(12, 0.0);
     active.assign(cs.size(), 1);
     stop_rc.assign(cs.size(), 0);
@@ -1891,6 +1902,13 @@ template <class T> struct BatchImpl : BatchBase {
     CK(cudaEventElapsedTime(&last_ms, ev0, ev1));
     int rc = 0;
     last_rc.assign(cs.size(), 0);
+    // the running cases' control blocks, then their last L2 residuals: one
+    // wait for each set of copies
+    auto running = [&](size_t i) { return active[i] && stop_rc[i] == 0; };
+    for (size_t i = 0; i < cs.size(); ++i)
+      if (running(i)) CK(cudaMemcpyAsync(&cs[i]->hctrl[1], cs[i]->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    std::vector<int> ns(cs.size(), 0);
     for (size_t i = 0; i < cs.size(); ++i) {
       Impl<T>* c = cs[i];
       if (steps) steps[i] = 0;
@@ -1901,17 +1919,21 @@ template <class T> struct BatchImpl : BatchBase {
         if (rc == 0) rc = stop_rc[i];
         continue;
       }
-      CK(cudaMemcpy(&c->hctrl[1], c->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost));
-      int ns = 0;
-      const int r = c->collect(c->hctrl[1], &ns, nullptr, nullptr, nullptr);
+      const int r = c->collect(c->hctrl[1], &ns[i], nullptr, nullptr, nullptr);
       last_rc[i] = r;
       if (r != 0) {
         stop_rc[i] = r;
         stop_epoch[i] = c->epoch;
         if (rc == 0) rc = r;
       }
-      if (steps) steps[i] = ns;
-      if (l2 && ns > 0) CK(cudaMemcpy(&l2[i], c->hist_l2 + ns - 1, sizeof(double), cudaMemcpyDeviceToHost));
+      if (steps) steps[i] = ns[i];
+      if (l2 && ns[i] > 0)
+        CK(cudaMemcpyAsync(&h_l2[i], c->hist_l2 + ns[i] - 1, sizeof(double), cudaMemcpyDeviceToHost, st));
+    }
+    if (l2) {
+      CK(cudaStreamSynchronize(st));
+      for (size_t i = 0; i < cs.size(); ++i)
+        if (ns[i] > 0) l2[i] = h_l2[i];
     }
     return rc;
   }

@@ -155,12 +155,14 @@ template <class T> struct alignas(64) CaseDev {
   unsigned rowbytes;  // V*sizeof(T) rounded up to 16
   // ALPHA < 1: the specular part of the wall flux (the host plan's tables)
   int spec;                 // 0: ALPHA = 1 or no wall side
+  int immat;                // 1: lumped mass (GETINC), 0: CMMINC
   int n_spec_par, n_spec_slots;
   const int* rside;         // [B] reflection-table row, -1 off the walls
   const int* rf_i;          // [rows][V][2] mirrored grid velocities I1, I2; -1 where TEST >= 0
   const T* rf_z;            // [rows][V][2] ZD1, ZD2
   const int* welem;         // [slots] wall elements (plan order)
-  T* wd;                    // [slots][3][Vp] deferred DELUN without the specular part
+  T* wd;                    // deferred values: IMMAT = 1 [slots][3][Vp] DELUN without the specular part;
+                            // IMMAT = 0 [2][slots][3][Vp] RHS*DTE without it, COLL*DTE
   const int* spec_par;      // items slot*V + v
   const int* spec_seq_off;  // [slots + 1]
   const int* spec_seq;
@@ -1311,12 +1313,13 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : (E
                 for (int i = 0; i < 3; ++i) {
                   const T f = VO::get(g[i], w) + u;
                   const T qmf = VO::get(qr[cc][i], w) - f;
-                  T d, rr;
+                  T d, rr, x = (T)0, cdt = (T)0;
                   if (IMMAT == 1) {
                     d = mmdt[i] * rhs[i][w] + mudt[i] * qmf;
                     rr = fabs(d);
                   } else {
-                    const T x = rhs[i][w] * dt, cdt = mudt[i] * qmf;
+                    x = rhs[i][w] * dt;
+                    cdt = mudt[i] * qmf;
                     d = r.mm[i] * x + cdt;
                     rr = ((x >= (T)0) ? cmx[i] : cmn[i]) * x + cdt;
                     rr = rr > (T)0 ? rr : (T)0;
@@ -1334,7 +1337,13 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : (E
                     if (decltype(defer)::value && ((dmask >> (3 * w + i)) & 1u)) {
                       // deferred: k_wspec adds the specular part, clips and
                       // counts the residual
-                      C.wd[((size_t)r.wslot * 3 + i) * C.Vp + vb + w] = d;
+                      const size_t o = ((size_t)r.wslot * 3 + i) * C.Vp + vb + w;
+                      if (IMMAT == 1) {
+                        C.wd[o] = d;
+                      } else {
+                        C.wd[o] = x;
+                        C.wd[(size_t)C.n_spec_slots * 3 * C.Vp + o] = cdt;
+                      }
                     } else {
                       rmt = fmax(rmt, rr);
                       if (!(flags & (1 << i))) sqt += ch * ch;
@@ -1435,16 +1444,18 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : (E
 }
 
 // ------------------------------------------------ specular wall part ----
-// GETBOU's specular part for ALPHA < 1 (src/getbou.f90:189-255, IMMAT = 1):
-// a molecule leaving wall side k of element e at velocity v carries
-// UNSID = (1-ALPHA)*Rf + ALPHA*ETA*Mw with Rf = (ZD2*f(I1) + ZD1*f(I2)) /
-// (ZD1 + ZD2) of the element's own nodes at the mirrored grid velocities.
-// The reference reads f(I) from DISNF while its velocity loop updates it in
+// GETBOU's specular part for ALPHA < 1 (src/getbou.f90:189-255): a molecule
+// leaving wall side k of element e at velocity v carries UNSID =
+// (1-ALPHA)*Rf + ALPHA*ETA*Mw with Rf = (ZD2*f(I1) + ZD1*f(I2)) / (ZD1 +
+// ZD2) of the element's own nodes at the mirrored grid velocities.  The
+// reference reads f(I) from DISNF while its velocity loop updates it in
 // place: the new value for I < v, the old one for I > v.  The sweep has
-// applied the diffuse part and stored DELUN of the deferred nodes (wd); the
-// specular part is linear in RHS, so here DELUN += MMAT*DTE*dRHS with dRHS
-// the edge term of (1-ALPHA)*Rf, then ADTHEM's clip, INFLOW's reset and the
-// residual.  seq = 0: the items whose mirrored velocities include no earlier
+// applied the diffuse part and stored the deferred nodes' partial update
+// (wd); the specular part is linear in RHS: with IMMAT = 1, DELUN +=
+// MMAT*DTE*dRHS with dRHS the edge term of (1-ALPHA)*Rf; with IMMAT = 0
+// CMMINC (src/cmminc.f90:22-41) on RHS*DTE + dRHS*DTE, its residual from the
+// CMMAT row's largest or smallest entry; then ADTHEM's clip, INFLOW's reset
+// and the residual.  seq = 0: the items whose mirrored velocities include no earlier
 // deferred one, a thread each; seq = 1: the others, one thread per wall
 // element in velocity order (after the parallel ones).
 template <class T> __global__ void __launch_bounds__(256) k_wspec(const __grid_constant__ CaseDev<T> C, int seq) {
@@ -1483,12 +1494,23 @@ template <class T> __global__ void __launch_bounds__(256) k_wspec(const __grid_c
     for (int i = 0; i < 3; ++i) {
       if (!((mask >> i) & 1u)) continue;
       const size_t o = ((size_t)e * 3 + i) * C.Vp + v;
-      const T d = C.wd[((size_t)s * 3 + i) * C.Vp + v] + (r.mm[i] * dt) * drhs[i];
+      const size_t od = ((size_t)s * 3 + i) * C.Vp + v;
+      T d, rr;
+      if (C.immat == 1) {
+        d = C.wd[od] + (r.mm[i] * dt) * drhs[i];
+        rr = fabs(d);
+      } else {
+        // CMMINC (src/cmminc.f90:22-41) on the whole RHS*DTE
+        const T x = C.wd[od] + dt * drhs[i], cdt = C.wd[(size_t)C.n_spec_slots * 3 * C.Vp + od];
+        d = r.mm[i] * x + cdt;
+        rr = ((x >= (T)0) ? C.cmax[3 * (size_t)e + i] : C.cmin[3 * (size_t)e + i]) * x + cdt;
+        rr = rr > (T)0 ? rr : (T)0;
+      }
       const T f = fo[o];
       T f1 = f + d;
       const T ch = (f1 < (T)0) ? -f : d;
       f1 = f1 > (T)0 ? f1 : (T)0;
-      mx = fmax(mx, (double)fabs(d));
+      mx = fmax(mx, (double)rr);
       if (r.flags & (1 << i))
         f1 = C.nfinf[v];
       else

@@ -457,8 +457,6 @@ int build_plan(const dgbgk_mesh& m, const dgbgk_vspace& vs, const dgbgk_params& 
   // ---- the specular part of the wall flux for ALPHA < 1
   pl.spec = false;
   if (p.alpha != 1.0 && pl.has_wall_incoming) {
-    if (p.immat != 1)
-      return fail(DGBGK_EUNSUP, "dgbgk_create: wall accommodation ALPHA < 1 needs IMMAT = 1 in this build");
     int rc = build_specular(m, vs, pl, err);
     if (rc != 0) return rc;
   }

@@ -111,3 +111,27 @@ def test_rre_driver_cycles_and_guard():
     assert worse.extrapolations == 1 and rel[1] <= 1e-8
     # m + 2 = 10 snapshots per cycle
     assert len(good.snaps) == 10 * good.extrapolations
+
+
+def test_rre_driver_confirms_a_warm_start_convergence():
+    # a transient whose residual dips to 1e-8 at step 3000, rises to 1e-5 at
+    # step 6000 and then decays for good (1e-8 again at step 9000)
+    def dip(k):
+        if k <= 3000:
+            return 10 ** (-k / 375)
+        if k <= 6000:
+            return 1e-8 * 10 ** ((k - 3000) / 1000)
+        return 1e-5 * 10 ** (-(k - 6000) / 1000)
+
+    plain = FakeCase(lambda k: 10 ** (-k / 500))   # 1e-8 at step 4000, falling
+    cases = [FakeCase(dip), FakeCase(dip), plain]
+    # without the confirmation the dip counts as convergence
+    steps, rel, status, _ = march_batch_rre(FakeBatch(cases[:1]), cases[:1], 1e-8, 60000, stall_below=0.0)
+    assert rel[0] <= 1e-8 and 3000 <= steps[0] < 3100
+    # with it the transient case marches on to its real convergence, and a
+    # case whose residual keeps falling stops `confirm` steps after its hit
+    steps, rel, status, _ = march_batch_rre(FakeBatch(cases[1:]), cases[1:], 1e-8, 60000, stall_below=0.0,
+                                            confirm=200)
+    assert rel[0] <= 1e-8 and 9000 <= steps[0] <= 9400
+    assert rel[1] <= 1e-8 and 4000 <= steps[1] <= 4300
+    assert (status == 0).all()

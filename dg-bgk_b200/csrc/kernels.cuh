@@ -941,7 +941,12 @@ __device__ __forceinline__ void resid_add(Ctrl* ctrl, const double* red_m, const
 //    per element (EDGFLXOPT src/edgflxopt.f90:95-125; outflow and, with zero
 //    length, inflow and wall sides read the element itself), the wall sides'
 //    fluxes (GETBOU src/getbou.f90:142-281), GETINC/CMMINC, ADTHEM and INFLOW;
-//    16-byte vector stores of the new rows.
+//    the new rows stay in registers.
+// Two barriers per tile: at the top (tile k has landed; every thread is
+// done with tile k - 1, whose new rows it then writes back into that tile's
+// buffer) and after phase 1; after the second, thread 0 stores tile k - 1
+// and the next tile's copies go into its buffer once the store has read it.
+// The unit's last tile is written back and stored at the unit's end.
 // ONE: a single case passed as a kernel parameter (its fields come from the
 // constant bank, no registers); otherwise the case table.
 // Upwinding: the own value is taken where SC = n.c > 0.  The reference takes
@@ -1088,6 +1093,11 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : (E
       // 3*EB ..) by cp.async, four threads per 64-byte row
       auto issue = [&](int vt, int bi) {
         unsigned char* dst = base + (size_t)bi * tile_bytes;
+        const T* src = C.f[cur] + (size_t)vt * VT;
+        for (int w = tid; w < nh * 12; w += NT) {
+          const int row = w >> 2, cq = w & 3;
+          cp_async16(dst + (tile_row_off(3 * EB + row) ^ (16u * cq)), src + (size_t)hrow[row] * C.Vp + cq * W);
+        }
         if (tid == 0) {
           bulk_wait_read0();
           fence_proxy_async_smem();  // the buffer's previous generic accesses
@@ -1096,13 +1106,24 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : (E
           for (int x = 0; x < NBOX; ++x)
             tma_load_2d(dst + x * BOX_BYTES, &C.tm[cur], vt * VT, 3 * e0 + x * G::BOX_ROWS, &bars[bi]);
         }
-        const T* src = C.f[cur] + (size_t)vt * VT;
-        for (int w = tid; w < nh * 12; w += NT) {
-          const int row = w >> 2, cq = w & 3;
-          cp_async16(dst + (tile_row_off(3 * EB + row) ^ (16u * cq)), src + (size_t)hrow[row] * C.Vp + cq * W);
-        }
       };
       const unsigned hx = 16u * CPT * hh;  // the thread's first chunk, as an offset XOR
+      // block element j's own rows at the thread's first chunk
+      unsigned own[3];
+#pragma unroll
+      for (int i = 0; i < 3; ++i) own[i] = tile_row_off(3 * j + i) ^ hx;
+      // the new rows of the previous tile, written back after the next
+      // tile's first barrier
+      VecT outv[CPT][3];
+      auto put_rows = [&](unsigned char* t) {
+        if (j < nb) {
+#pragma unroll
+          for (int cc = 0; cc < CPT; ++cc)
+#pragma unroll
+            for (int i = 0; i < 3; ++i) vst<T>(t + (own[i] ^ (16u * cc)), outv[cc][i]);
+        }
+        fence_proxy_async_smem();
+      };
 
       for (int k = 0; k < ntl; ++k, ++gk) {
         const int bi = gk & 1;
@@ -1121,17 +1142,15 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : (E
           break;
         }
         if (tid != 0) mbar_try_wait(&bars[bi], ph);  // completed: acquires the box data
-        if (tid == 0 && k > 0) store(&C.tm[cur ^ 1], vt0 + k - 1, bi ^ 1, 3 * e0);
+        // every thread is past its phase-2 reads of tile k - 1: its new rows
+        // replace the block rows in its buffer, for the box store
+        if (k > 0) put_rows(base + (size_t)(bi ^ 1) * tile_bytes);
         const int vb0 = (vt0 + k) * VT;
         const T* vx = vtab + k * VT;
         const T* vy = vtab + UV + k * VT;
         const T* vn = vtab + 2 * UV + k * VT;
         const T* vc2 = vtab + (G::NTAB - 1) * UV + k * VT;  // |c|^2 (FP64; unused in FP32)
 
-        // block element j's own rows at the thread's first chunk
-        unsigned own[3];
-#pragma unroll
-        for (int i = 0; i < 3; ++i) own[i] = tile_row_off(3 * j + i) ^ hx;
         // ---- phase 1: block element j (chunks CPT*hh ..), then the halo
         // chunk by chunk
         VecT qr[CPT][3], ur[CPT];
@@ -1156,7 +1175,9 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : (E
                       ud);
         }
         __syncthreads();
-        // the other buffer's tile k - 1 is stored (or being stored): load tile k + 1
+        // tile k - 1's new rows are in place: store them, then load tile k + 1
+        // into that buffer once the store has read it
+        if (tid == 0 && k > 0) store(&C.tm[cur ^ 1], vt0 + k - 1, bi ^ 1, 3 * e0);
         if (k + 1 < ntl) {
           issue(vt0 + k + 1, bi ^ 1);
           cp_async_commit();
@@ -1166,7 +1187,6 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : (E
         // CPT*hh + CPT - 1 (row offsets own[], srcp[], srcq[] are at chunk
         // CPT*hh; chunk CPT*hh + cc of the same row is at offset ^ 16*cc)
         T rmt = (T)0, sqt = (T)0;
-        VecT outv[CPT][3];
         if (j < nb) {
           const ElemRec<T>& r = recs[j];
           // per edge: the flux source's rows, AL*n where the edge carries
@@ -1376,16 +1396,6 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : (E
         }
         rmax = fmax(rmax, (double)rmt);
         rsq += (double)sqt;
-        // every thread is past its phase-2 reads of tile k: the new rows
-        // replace the block rows in the buffer, for the box store
-        __syncthreads();
-        if (j < nb) {
-#pragma unroll
-          for (int cc = 0; cc < CPT; ++cc)
-#pragma unroll
-            for (int i = 0; i < 3; ++i) vst<T>(tl + (own[i] ^ (16u * cc)), outv[cc][i]);
-        }
-        fence_proxy_async_smem();
       }
       if (aborted) {
         // a bounded wait expired (the vote made every thread leave the tile
@@ -1412,6 +1422,9 @@ __global__ void __launch_bounds__(SweepGeo<T>::TPE * EB, sizeof(T) == 4 ? 2 : (E
       last_vt = vt0 + ntl - 1;
       last_bi = (gk - 1) & 1;
       last_y0 = 3 * e0;
+      // the last tile's new rows, once every thread is past its reads
+      __syncthreads();
+      put_rows(base + (size_t)last_bi * tile_bytes);
     }
     // every thread is past phase 2 of the unit's last tile and has written
     // its rows: store the last tile and (a batch) add the unit's residual to

@@ -134,7 +134,25 @@ template <class T> struct LaunchSet {
   std::vector<CaseDev<T>> spec_cases;  // cases with ALPHA < 1 wall sides (k_wspec runs per case)
   int mom_rows = 1, mom_warps = 1, mom_grid = 1, sweep_grid = 1;
   size_t mom_smem = 0, sweep_smem = 0;
-  ~LaunchSet() { release(); }
+  // the wall kernel's branch: it runs beside the moment kernel (both read
+  // the state only; the sweep reads the wall's ETA and waits for both)
+  cudaStream_t st_wall = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  LaunchSet() = default;
+  LaunchSet(const LaunchSet&) = delete;
+  LaunchSet& operator=(const LaunchSet&) = delete;
+  ~LaunchSet() {
+    release();
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+    if (st_wall) cudaStreamDestroy(st_wall);
+  }
+  int ensure_wall_branch() {
+    if (!st_wall) CK(cudaStreamCreateWithFlags(&st_wall, cudaStreamNonBlocking));
+    if (!ev_fork) CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+    if (!ev_join) CK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+    return 0;
+  }
   void release() {
     dfree(d_cases);
     dfree(d_off);
@@ -299,6 +317,7 @@ int build_launch_set(LaunchSet<T>& L, const std::vector<CaseDev<T>>& cs, int eb,
   L.total_units = off[n];
   L.total_groups = off[(n + 1) + n];
   L.total_walls = off[2 * (n + 1) + n];
+  if (L.total_walls > 0) TRY(L.ensure_wall_branch());
   L.args.cases = L.d_cases;
   L.args.unit_off = L.d_off;
   L.args.grp_off = L.d_off + (n + 1);
@@ -343,6 +362,16 @@ int enqueue_step(const LaunchSet<T>& L, cudaStream_t st, float* ms = nullptr, co
   if (ms)
     for (auto& e : ev) CK(cudaEventCreate(&e));
   if (ms) cudaEventRecord(ev[0], st);
+  // the wall flux on its own branch beside the moments (not when timing the
+  // kernels one by one)
+  const bool branch = !ms && L.total_walls > 0 && L.st_wall;
+  if (branch) {
+    CK(cudaEventRecord(L.ev_fork, st));
+    CK(cudaStreamWaitEvent(L.st_wall, L.ev_fork, 0));
+    k_wall<T><<<L.total_walls, WALL_THREADS, 0, L.st_wall>>>(L.args, L.total_walls);
+    TRY(launch_check("k_wall", L.total_walls, WALL_THREADS, 0));
+    CK(cudaEventRecord(L.ev_join, L.st_wall));
+  }
   mom_fn<T>(L.mom_rows, L.one)<<<L.mom_grid, L.mom_warps * 32, L.mom_smem, st>>>(L.args, L.total_groups,
                                                                                  L.one_case);
   TRY(launch_check("k_moments", L.mom_grid, L.mom_warps * 32, L.mom_smem));
@@ -354,7 +383,9 @@ int enqueue_step(const LaunchSet<T>& L, cudaStream_t st, float* ms = nullptr, co
     TRY(launch_check("k_out_forces", 1, FORCE_THREADS, 0));
   }
   if (ms) cudaEventRecord(ev[1], st);
-  if (L.total_walls > 0) {
+  if (branch) {
+    CK(cudaStreamWaitEvent(st, L.ev_join, 0));
+  } else if (L.total_walls > 0) {
     k_wall<T><<<L.total_walls, WALL_THREADS, 0, st>>>(L.args, L.total_walls);
     TRY(launch_check("k_wall", L.total_walls, WALL_THREADS, 0));
   }

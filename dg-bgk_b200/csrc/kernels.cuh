@@ -757,7 +757,7 @@ template <class T> struct SweepGeo {
     return ((size_t)3 * (EB + max_halo) * 64 + 1023) / 1024 * 1024;
   }
   // alignment slack, two tiles, records [EB], halo heads [max_halo][HR],
-  // velocity tables cx, cy, NFINF [3][TPU_MAX * VT], halo element list
+  // velocity tables [NTAB][TPU_MAX * VT], halo row list [3 * max_halo]
   static constexpr size_t smem(int EB, int max_halo) {
     return 1024 + 2 * tile_bytes(EB, max_halo) + (size_t)EB * sizeof(ElemRec<T>) + (size_t)max_halo * HR +
            NTAB * (size_t)TPU_MAX * VT * sizeof(T) + ((size_t)3 * max_halo * 4 + 15) / 16 * 16;

@@ -338,6 +338,9 @@ template <> struct RowMath<float> {
 template <class T> struct ElemMath;
 
 template <> struct ElemMath<float> {
+  // Each sum runs as two partial sums (the even and the odd values of a
+  // vector: shorter dependent chains; measured 0.1535 -> 0.1508 ms on the
+  // 200x100 channel; four partials were slower).
   // pass 1.  TAB: from the tables w, w*cx, w*cy (three FMAs per value;
   // tables in shared memory); otherwise from w, cx, cy (w*f, then three
   // sums; the tables the second pass reads too, through L1)
@@ -347,16 +350,19 @@ template <> struct ElemMath<float> {
     const float4* wj = reinterpret_cast<const float4*>(tb + 2 * Vp);
     const float4* wx = reinterpret_cast<const float4*>(tb + (TAB ? 3 : 0) * Vp);
     const float4* wy = reinterpret_cast<const float4*>(tb + (TAB ? 4 : 1) * Vp);
-    float t[3][3] = {};
+    float t[3][3] = {}, t2[3][3] = {};
     for (int q = lane; q < nq; q += 32) {
       const float4 w = wj[q], c = wx[q], d = wy[q];
 #pragma unroll
       for (int r = 0; r < 3; ++r) {
         const float4 x = reinterpret_cast<const float4*>(reinterpret_cast<const unsigned char*>(rows) + r * pitch)[q];
         if constexpr (TAB) {
-          t[r][0] = fmaf(w.x, x.x, fmaf(w.y, x.y, fmaf(w.z, x.z, fmaf(w.w, x.w, t[r][0]))));
-          t[r][1] = fmaf(c.x, x.x, fmaf(c.y, x.y, fmaf(c.z, x.z, fmaf(c.w, x.w, t[r][1]))));
-          t[r][2] = fmaf(d.x, x.x, fmaf(d.y, x.y, fmaf(d.z, x.z, fmaf(d.w, x.w, t[r][2]))));
+          t[r][0] = fmaf(w.x, x.x, fmaf(w.z, x.z, t[r][0]));
+          t2[r][0] = fmaf(w.y, x.y, fmaf(w.w, x.w, t2[r][0]));
+          t[r][1] = fmaf(c.x, x.x, fmaf(c.z, x.z, t[r][1]));
+          t2[r][1] = fmaf(c.y, x.y, fmaf(c.w, x.w, t2[r][1]));
+          t[r][2] = fmaf(d.x, x.x, fmaf(d.z, x.z, t[r][2]));
+          t2[r][2] = fmaf(d.y, x.y, fmaf(d.w, x.w, t2[r][2]));
         } else {
           const float a0 = w.x * x.x, a1 = w.y * x.y, a2 = w.z * x.z, a3 = w.w * x.w;
           t[r][0] += (a0 + a1) + (a2 + a3);
@@ -368,14 +374,14 @@ template <> struct ElemMath<float> {
 #pragma unroll
     for (int r = 0; r < 3; ++r)
 #pragma unroll
-      for (int k = 0; k < 3; ++k) s[r][k] = (double)t[r][k];
+      for (int k = 0; k < 3; ++k) s[r][k] = (double)t[r][k] + (double)t2[r][k];
   }
   static __device__ __forceinline__ void pass2(const float* rows, unsigned pitch, const float* tb, int Vp, int nq,
                                                int lane, const double (&u)[3][2], double (&s)[3][2]) {
     const float4* cx = reinterpret_cast<const float4*>(tb);
     const float4* cy = reinterpret_cast<const float4*>(tb + Vp);
     const float4* wj = reinterpret_cast<const float4*>(tb + 2 * Vp);
-    float fu[3][2], t[3][2] = {};
+    float fu[3][2], t[3][2] = {}, t2[3][2] = {};
 #pragma unroll
     for (int r = 0; r < 3; ++r) {
       fu[r][0] = (float)u[r][0];
@@ -391,15 +397,16 @@ template <> struct ElemMath<float> {
         const float q0 = fmaf(e0, e0, g0 * g0), q1 = fmaf(e1, e1, g1 * g1), q2 = fmaf(e2, e2, g2 * g2),
                     q3 = fmaf(e3, e3, g3 * g3);
         const float a0 = w.x * x.x, a1 = w.y * x.y, a2 = w.z * x.z, a3 = w.w * x.w;
-        t[r][0] = fmaf(q0, a0, fmaf(q1, a1, fmaf(q2, a2, fmaf(q3, a3, t[r][0]))));  // src/macros.f90:144-148
-        t[r][1] = fmaf(sqrt_fast(q0), a0,
-                       fmaf(sqrt_fast(q1), a1, fmaf(sqrt_fast(q2), a2, fmaf(sqrt_fast(q3), a3, t[r][1]))));
+        t[r][0] = fmaf(q0, a0, fmaf(q2, a2, t[r][0]));  // src/macros.f90:144-148
+        t2[r][0] = fmaf(q1, a1, fmaf(q3, a3, t2[r][0]));
+        t[r][1] = fmaf(sqrt_fast(q0), a0, fmaf(sqrt_fast(q2), a2, t[r][1]));
+        t2[r][1] = fmaf(sqrt_fast(q1), a1, fmaf(sqrt_fast(q3), a3, t2[r][1]));
       }
     }
 #pragma unroll
     for (int r = 0; r < 3; ++r) {
-      s[r][0] = 0.5 * (double)t[r][0];
-      s[r][1] = (double)t[r][1];
+      s[r][0] = 0.5 * ((double)t[r][0] + (double)t2[r][0]);
+      s[r][1] = (double)t[r][1] + (double)t2[r][1];
     }
   }
 };

@@ -257,7 +257,7 @@ int build_launch_set(LaunchSet<T>& L, const std::vector<CaseDev<T>>& cs, int eb,
   const size_t cap = 227 * 1024;
   long best = -1;
   for (int R : {4, 3, 2, 1})
-    for (int w : {20, 16, 12, 10, 8, 6, 5, 4, 3, 2, 1})
+    for (int w : {20, 16, 15, 14, 13, 12, 10, 8, 6, 5, 4, 3, 2, 1})
       for (int sg : {3, 2, 1}) {
         if (force_rows > 0 && R != force_rows) continue;
         const size_t tbytes = one ? (mom_tables(R) * (size_t)cs[0].Vp * sizeof(T) + 127) / 128 * 128 : 0;

@@ -289,45 +289,51 @@ template <> struct RowMath<double> {
   }
 };
 
+__device__ __forceinline__ float2 lo2(const float4& v) { return make_float2(v.x, v.y); }
+__device__ __forceinline__ float2 hi2(const float4& v) { return make_float2(v.z, v.w); }
+
 template <> struct RowMath<float> {
+  // on packed pairs (fma/add/mul.rn.f32x2): each sum as two partial sums,
+  // the halves of one pair (the even and the odd values of a vector)
   static __device__ __forceinline__ void pass1(const float* row, const float* tb, int Vp, int nq, int sub, int L,
                                                double& s0, double& s1, double& s2) {
     const float4* r = reinterpret_cast<const float4*>(row);
     const float4* cx = reinterpret_cast<const float4*>(tb);
     const float4* cy = reinterpret_cast<const float4*>(tb + Vp);
     const float4* wj = reinterpret_cast<const float4*>(tb + 2 * Vp);
-    float t0 = 0.f, t1 = 0.f, t2 = 0.f;
+    float2 t0 = make_float2(0.f, 0.f), t1 = t0, t2 = t0;
     for (int q = sub; q < nq; q += L) {
       const float4 x = r[q], c = cx[q], d = cy[q], w = wj[q];
-      const float a0 = w.x * x.x, a1 = w.y * x.y, a2 = w.z * x.z, a3 = w.w * x.w;
-      t0 += (a0 + a1) + (a2 + a3);
-      t1 = fmaf(c.x, a0, fmaf(c.y, a1, fmaf(c.z, a2, fmaf(c.w, a3, t1))));
-      t2 = fmaf(d.x, a0, fmaf(d.y, a1, fmaf(d.z, a2, fmaf(d.w, a3, t2))));
+      const float2 al = __fmul2_rn(lo2(w), lo2(x)), ah = __fmul2_rn(hi2(w), hi2(x));
+      t0 = __fadd2_rn(t0, __fadd2_rn(al, ah));
+      t1 = __ffma2_rn(lo2(c), al, __ffma2_rn(hi2(c), ah, t1));
+      t2 = __ffma2_rn(lo2(d), al, __ffma2_rn(hi2(d), ah, t2));
     }
-    s0 += (double)t0;
-    s1 += (double)t1;
-    s2 += (double)t2;
+    s0 += (double)t0.x + (double)t0.y;
+    s1 += (double)t1.x + (double)t1.y;
+    s2 += (double)t2.x + (double)t2.y;
   }
   static __device__ __forceinline__ void pass2(const float* row, const float* tb, int Vp, int nq, int sub, int L,
                                                double ux, double uy, double& sp, double& sc) {
-    const float fx = (float)ux, fy = (float)uy;
+    const float2 nx = make_float2(-(float)ux, -(float)ux), ny = make_float2(-(float)uy, -(float)uy);
     const float4* r = reinterpret_cast<const float4*>(row);
     const float4* cx = reinterpret_cast<const float4*>(tb);
     const float4* cy = reinterpret_cast<const float4*>(tb + Vp);
     const float4* wj = reinterpret_cast<const float4*>(tb + 2 * Vp);
-    float tp = 0.f, tc = 0.f;
+    float2 tp = make_float2(0.f, 0.f), tc = tp;
     for (int q = sub; q < nq; q += L) {
       const float4 x = r[q], c = cx[q], d = cy[q], w = wj[q];
-      const float e0 = c.x - fx, e1 = c.y - fx, e2 = c.z - fx, e3 = c.w - fx;
-      const float g0 = d.x - fy, g1 = d.y - fy, g2 = d.z - fy, g3 = d.w - fy;
-      const float q0 = fmaf(e0, e0, g0 * g0), q1 = fmaf(e1, e1, g1 * g1), q2 = fmaf(e2, e2, g2 * g2),
-                  q3 = fmaf(e3, e3, g3 * g3);
-      const float a0 = w.x * x.x, a1 = w.y * x.y, a2 = w.z * x.z, a3 = w.w * x.w;
-      tp = fmaf(q0, a0, fmaf(q1, a1, fmaf(q2, a2, fmaf(q3, a3, tp))));
-      tc = fmaf(sqrt_fast(q0), a0, fmaf(sqrt_fast(q1), a1, fmaf(sqrt_fast(q2), a2, fmaf(sqrt_fast(q3), a3, tc))));
+      const float2 el = __fadd2_rn(lo2(c), nx), eh = __fadd2_rn(hi2(c), nx);
+      const float2 gl = __fadd2_rn(lo2(d), ny), gh = __fadd2_rn(hi2(d), ny);
+      const float2 ql = __ffma2_rn(el, el, __fmul2_rn(gl, gl)), qh = __ffma2_rn(eh, eh, __fmul2_rn(gh, gh));
+      const float2 al = __fmul2_rn(lo2(w), lo2(x)), ah = __fmul2_rn(hi2(w), hi2(x));
+      tp = __ffma2_rn(ql, al, __ffma2_rn(qh, ah, tp));
+      const float2 sl = make_float2(sqrt_fast(ql.x), sqrt_fast(ql.y));
+      const float2 sh = make_float2(sqrt_fast(qh.x), sqrt_fast(qh.y));
+      tc = __ffma2_rn(sl, al, __ffma2_rn(sh, ah, tc));
     }
-    sp += 0.5 * (double)tp;
-    sc += (double)tc;
+    sp += 0.5 * ((double)tp.x + (double)tp.y);
+    sc += (double)tc.x + (double)tc.y;
   }
 };
 
@@ -338,9 +344,12 @@ template <> struct RowMath<float> {
 template <class T> struct ElemMath;
 
 template <> struct ElemMath<float> {
-  // Each sum runs as two partial sums (the even and the odd values of a
-  // vector: shorter dependent chains; measured 0.1535 -> 0.1508 ms on the
-  // 200x100 channel; four partials were slower).
+  // Each sum runs as two partial sums, the even and the odd values of a
+  // vector (shorter dependent chains: 0.1535 -> 0.1508 ms on the 200x100
+  // channel; four partials were slower).  Where the two partial sums take
+  // the same operations, they are the halves of one packed pair
+  // (fma/add/mul.rn.f32x2: one instruction for two values; the same bits
+  // as two scalar chains; 0.1527 -> 0.1456 ms).
   // pass 1.  TAB: from the tables w, w*cx, w*cy (three FMAs per value;
   // tables in shared memory); otherwise from w, cx, cy (w*f, then three
   // sums; the tables the second pass reads too, through L1)
@@ -350,63 +359,80 @@ template <> struct ElemMath<float> {
     const float4* wj = reinterpret_cast<const float4*>(tb + 2 * Vp);
     const float4* wx = reinterpret_cast<const float4*>(tb + (TAB ? 3 : 0) * Vp);
     const float4* wy = reinterpret_cast<const float4*>(tb + (TAB ? 4 : 1) * Vp);
-    float t[3][3] = {}, t2[3][3] = {};
-    for (int q = lane; q < nq; q += 32) {
-      const float4 w = wj[q], c = wx[q], d = wy[q];
+    if constexpr (TAB) {
+      float2 t[3][3];
 #pragma unroll
-      for (int r = 0; r < 3; ++r) {
-        const float4 x = reinterpret_cast<const float4*>(reinterpret_cast<const unsigned char*>(rows) + r * pitch)[q];
-        if constexpr (TAB) {
-          t[r][0] = fmaf(w.x, x.x, fmaf(w.z, x.z, t[r][0]));
-          t2[r][0] = fmaf(w.y, x.y, fmaf(w.w, x.w, t2[r][0]));
-          t[r][1] = fmaf(c.x, x.x, fmaf(c.z, x.z, t[r][1]));
-          t2[r][1] = fmaf(c.y, x.y, fmaf(c.w, x.w, t2[r][1]));
-          t[r][2] = fmaf(d.x, x.x, fmaf(d.z, x.z, t[r][2]));
-          t2[r][2] = fmaf(d.y, x.y, fmaf(d.w, x.w, t2[r][2]));
-        } else {
+      for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) t[r][k] = make_float2(0.f, 0.f);
+      for (int q = lane; q < nq; q += 32) {
+        const float4 w = wj[q], c = wx[q], d = wy[q];
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+          const float4 x =
+              reinterpret_cast<const float4*>(reinterpret_cast<const unsigned char*>(rows) + r * pitch)[q];
+          t[r][0] = __ffma2_rn(lo2(w), lo2(x), __ffma2_rn(hi2(w), hi2(x), t[r][0]));
+          t[r][1] = __ffma2_rn(lo2(c), lo2(x), __ffma2_rn(hi2(c), hi2(x), t[r][1]));
+          t[r][2] = __ffma2_rn(lo2(d), lo2(x), __ffma2_rn(hi2(d), hi2(x), t[r][2]));
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) s[r][k] = (double)t[r][k].x + (double)t[r][k].y;
+    } else {
+      float t[3][3] = {};
+      for (int q = lane; q < nq; q += 32) {
+        const float4 w = wj[q], c = wx[q], d = wy[q];
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+          const float4 x =
+              reinterpret_cast<const float4*>(reinterpret_cast<const unsigned char*>(rows) + r * pitch)[q];
           const float a0 = w.x * x.x, a1 = w.y * x.y, a2 = w.z * x.z, a3 = w.w * x.w;
           t[r][0] += (a0 + a1) + (a2 + a3);
           t[r][1] = fmaf(c.x, a0, fmaf(c.y, a1, fmaf(c.z, a2, fmaf(c.w, a3, t[r][1]))));
           t[r][2] = fmaf(d.x, a0, fmaf(d.y, a1, fmaf(d.z, a2, fmaf(d.w, a3, t[r][2]))));
         }
       }
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) s[r][k] = (double)t[r][k];
     }
-#pragma unroll
-    for (int r = 0; r < 3; ++r)
-#pragma unroll
-      for (int k = 0; k < 3; ++k) s[r][k] = (double)t[r][k] + (double)t2[r][k];
   }
+  // pass 2 on packed pairs (c - u as c + (-u))
   static __device__ __forceinline__ void pass2(const float* rows, unsigned pitch, const float* tb, int Vp, int nq,
                                                int lane, const double (&u)[3][2], double (&s)[3][2]) {
     const float4* cx = reinterpret_cast<const float4*>(tb);
     const float4* cy = reinterpret_cast<const float4*>(tb + Vp);
     const float4* wj = reinterpret_cast<const float4*>(tb + 2 * Vp);
-    float fu[3][2], t[3][2] = {}, t2[3][2] = {};
+    float2 nu[3][2], t[3][2];
 #pragma unroll
     for (int r = 0; r < 3; ++r) {
-      fu[r][0] = (float)u[r][0];
-      fu[r][1] = (float)u[r][1];
+      const float ux = (float)u[r][0], uy = (float)u[r][1];
+      nu[r][0] = make_float2(-ux, -ux);
+      nu[r][1] = make_float2(-uy, -uy);
+      t[r][0] = t[r][1] = make_float2(0.f, 0.f);
     }
     for (int q = lane; q < nq; q += 32) {
       const float4 c = cx[q], d = cy[q], w = wj[q];
 #pragma unroll
       for (int r = 0; r < 3; ++r) {
         const float4 x = reinterpret_cast<const float4*>(reinterpret_cast<const unsigned char*>(rows) + r * pitch)[q];
-        const float e0 = c.x - fu[r][0], e1 = c.y - fu[r][0], e2 = c.z - fu[r][0], e3 = c.w - fu[r][0];
-        const float g0 = d.x - fu[r][1], g1 = d.y - fu[r][1], g2 = d.z - fu[r][1], g3 = d.w - fu[r][1];
-        const float q0 = fmaf(e0, e0, g0 * g0), q1 = fmaf(e1, e1, g1 * g1), q2 = fmaf(e2, e2, g2 * g2),
-                    q3 = fmaf(e3, e3, g3 * g3);
-        const float a0 = w.x * x.x, a1 = w.y * x.y, a2 = w.z * x.z, a3 = w.w * x.w;
-        t[r][0] = fmaf(q0, a0, fmaf(q2, a2, t[r][0]));  // src/macros.f90:144-148
-        t2[r][0] = fmaf(q1, a1, fmaf(q3, a3, t2[r][0]));
-        t[r][1] = fmaf(sqrt_fast(q0), a0, fmaf(sqrt_fast(q2), a2, t[r][1]));
-        t2[r][1] = fmaf(sqrt_fast(q1), a1, fmaf(sqrt_fast(q3), a3, t2[r][1]));
+        const float2 el = __fadd2_rn(lo2(c), nu[r][0]), eh = __fadd2_rn(hi2(c), nu[r][0]);
+        const float2 gl = __fadd2_rn(lo2(d), nu[r][1]), gh = __fadd2_rn(hi2(d), nu[r][1]);
+        const float2 ql = __ffma2_rn(el, el, __fmul2_rn(gl, gl)), qh = __ffma2_rn(eh, eh, __fmul2_rn(gh, gh));
+        const float2 al = __fmul2_rn(lo2(w), lo2(x)), ah = __fmul2_rn(hi2(w), hi2(x));
+        t[r][0] = __ffma2_rn(ql, al, __ffma2_rn(qh, ah, t[r][0]));  // src/macros.f90:144-148
+        const float2 sl = make_float2(sqrt_fast(ql.x), sqrt_fast(ql.y));
+        const float2 sh = make_float2(sqrt_fast(qh.x), sqrt_fast(qh.y));
+        t[r][1] = __ffma2_rn(sl, al, __ffma2_rn(sh, ah, t[r][1]));  // src/compmu.f90:71-74
       }
     }
 #pragma unroll
     for (int r = 0; r < 3; ++r) {
-      s[r][0] = 0.5 * ((double)t[r][0] + (double)t2[r][0]);
-      s[r][1] = (double)t[r][1] + (double)t2[r][1];
+      s[r][0] = 0.5 * ((double)t[r][0].x + (double)t[r][0].y);
+      s[r][1] = (double)t[r][1].x + (double)t[r][1].y;
     }
   }
 };

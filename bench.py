@@ -426,7 +426,8 @@ def run_ours(a, d):
                              "loss_last": float(hist[-50:].mean())}}
         for k, name in (("fast_cold_rre", "fast_cold_rre"), ("fast_rre", "fast_warm_rre")):
             e = res[k]["rel_l2_vs_plain"]
-            st[name] = {"wall_s": res[k]["wall_s"], "speedup_vs_plain": res[k]["speedup_vs_plain"],
+            st[name] = {"wall_s": res[k]["wall_s"], "device_s": res[k]["device_s"],
+                        "speedup_vs_plain": res[k]["speedup_vs_plain"],
                         "steps": int(sum(res[k]["steps"])), "steps_fp64_finish": int(sum(res[k]["steps_fp64_finish"])),
                         "max_rel_l2_vs_plain": res[k]["max_rel_l2_vs_plain"],
                         "cases_over_1e-6": int(sum(max(x["n"], x["u"], x["T"]) > 1e-6 for x in e)),

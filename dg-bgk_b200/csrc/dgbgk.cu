@@ -420,6 +420,52 @@ int enqueue_step(const LaunchSet<T>& L, cudaStream_t st, float* ms = nullptr, co
   return 0;
 }
 
+// Reduced-rank extrapolation coefficients from the m x m Gram matrix G of
+// the snapshot differences (upper triangle accumulated by k_gram): solve
+// G gamma = 1 and scale to sum(gamma) = 1.  G is overwritten.
+int rre_coeffs(std::vector<double>& G, int m, std::vector<double>& g) {
+  // G gamma = 1 (upper triangle accumulated), a tiny ridge, Gaussian
+  // elimination with partial pivoting, then sum(gamma) = 1
+  double tr = 0;
+  for (int a = 0; a < m; ++a) {
+    for (int b = 0; b < a; ++b) G[a * m + b] = G[b * m + a];
+    tr += G[a * m + a];
+  }
+  if (!(tr > 0) || !std::isfinite(tr)) {
+    set_error("dgbgk_extrapolate: the snapshots do not differ");
+    return DGBGK_EINVAL;
+  }
+  for (int a = 0; a < m; ++a) G[a * m + a] += 1e-14 * tr;
+  g.assign(m, 1.0);
+  for (int c = 0; c < m; ++c) {
+    int pv = c;
+    for (int r = c + 1; r < m; ++r)
+      if (std::fabs(G[r * m + c]) > std::fabs(G[pv * m + c])) pv = r;
+    if (pv != c) {
+      for (int k = 0; k < m; ++k) std::swap(G[c * m + k], G[pv * m + k]);
+      std::swap(g[c], g[pv]);
+    }
+    for (int r = c + 1; r < m; ++r) {
+      const double fct = G[r * m + c] / G[c * m + c];
+      for (int k = c; k < m; ++k) G[r * m + k] -= fct * G[c * m + k];
+      g[r] -= fct * g[c];
+    }
+  }
+  for (int c = m - 1; c >= 0; --c) {
+    for (int k = c + 1; k < m; ++k) g[c] -= G[c * m + k] * g[k];
+    g[c] /= G[c * m + c];
+  }
+  double sum = 0;
+  for (double x : g) sum += x;
+  for (auto& x : g) x /= sum;
+  for (double x : g)
+    if (!std::isfinite(x)) {
+      set_error("dgbgk_extrapolate: singular difference system");
+      return DGBGK_ENONFINITE;
+    }
+  return 0;
+}
+
 template <class T> struct Impl : ImplBase {
   static constexpr int GRAPH_STEPS = 2;  // pseudo-time steps per graph launch
   cudaStream_t st = nullptr;
@@ -1115,6 +1161,21 @@ template <class T> struct Impl : ImplBase {
     itime_total = 0;  // a new state: ITIME starts again
     return 0;
   }
+  // room for `cap` snapshot slots, keeping the slots taken so far (the
+  // caller has let every queued copy into them finish)
+  int grow_snaps(int cap) {
+    const size_t N = (size_t)3 * pl.E * Vp;
+    T* nb = nullptr;
+    CK(cudaMalloc((void**)&nb, (size_t)cap * N * sizeof(T)));
+    if (snaps) {
+      CK(cudaMemcpyAsync(nb, snaps, (size_t)snap_cap * N * sizeof(T), cudaMemcpyDeviceToDevice, st));
+      CK(cudaStreamSynchronize(st));
+      cudaFree(snaps);
+    }
+    snaps = nb;
+    snap_cap = cap;
+    return 0;
+  }
   int snapshot(int slot) override {
     CK(cudaSetDevice(device));
     const size_t N = (size_t)3 * pl.E * Vp;
@@ -1128,17 +1189,7 @@ template <class T> struct Impl : ImplBase {
       set_error("dgbgk_snapshot: slot beyond the extrapolation limit of " + std::to_string(RRE_MAX) + " snapshots");
       return DGBGK_EINVAL;
     }
-    if (slot >= snap_cap) {  // grow, keeping the slots taken so far
-      T* nb = nullptr;
-      CK(cudaMalloc((void**)&nb, (size_t)(slot + 1) * N * sizeof(T)));
-      if (snaps) {
-        CK(cudaMemcpyAsync(nb, snaps, (size_t)snap_cap * N * sizeof(T), cudaMemcpyDeviceToDevice, st));
-        CK(cudaStreamSynchronize(st));
-        cudaFree(snaps);
-      }
-      snaps = nb;
-      snap_cap = slot + 1;
-    }
+    if (slot >= snap_cap) TRY(grow_snaps(slot + 1));
     // waited for: measured on the bench's eight channels, leaving the copy
     // queued on the case's stream made the extrapolated march slower (the
     // snapshot calls 0.20 -> 0.43 ms each)
@@ -1160,48 +1211,10 @@ template <class T> struct Impl : ImplBase {
     const int grid = (int)std::min<size_t>((size_t)4 * nsm, (N + 255) / 256);
     k_gram<T><<<grid, 256, 0, st>>>(snaps, N, n, N, d_gram);
     CK(cudaGetLastError());
-    std::vector<double> G((size_t)m * m);
+    std::vector<double> G((size_t)m * m), g;
     CK(cudaMemcpyAsync(G.data(), d_gram, G.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
-    // G gamma = 1 (upper triangle accumulated), a tiny ridge, Gaussian
-    // elimination with partial pivoting, then sum(gamma) = 1
-    double tr = 0;
-    for (int a = 0; a < m; ++a) {
-      for (int b = 0; b < a; ++b) G[a * m + b] = G[b * m + a];
-      tr += G[a * m + a];
-    }
-    if (!(tr > 0) || !std::isfinite(tr)) {
-      set_error("dgbgk_extrapolate: the snapshots do not differ");
-      return DGBGK_EINVAL;
-    }
-    for (int a = 0; a < m; ++a) G[a * m + a] += 1e-14 * tr;
-    std::vector<double> g(m, 1.0);
-    for (int c = 0; c < m; ++c) {
-      int pv = c;
-      for (int r = c + 1; r < m; ++r)
-        if (std::fabs(G[r * m + c]) > std::fabs(G[pv * m + c])) pv = r;
-      if (pv != c) {
-        for (int k = 0; k < m; ++k) std::swap(G[c * m + k], G[pv * m + k]);
-        std::swap(g[c], g[pv]);
-      }
-      for (int r = c + 1; r < m; ++r) {
-        const double fct = G[r * m + c] / G[c * m + c];
-        for (int k = c; k < m; ++k) G[r * m + k] -= fct * G[c * m + k];
-        g[r] -= fct * g[c];
-      }
-    }
-    for (int c = m - 1; c >= 0; --c) {
-      for (int k = c + 1; k < m; ++k) g[c] -= G[c * m + k] * g[k];
-      g[c] /= G[c * m + c];
-    }
-    double sum = 0;
-    for (double x : g) sum += x;
-    for (auto& x : g) x /= sum;
-    for (double x : g)
-      if (!std::isfinite(x)) {
-        set_error("dgbgk_extrapolate: singular difference system");
-        return DGBGK_ENONFINITE;
-      }
+    TRY(rre_coeffs(G, m, g));
     if (gamma) std::copy(g.begin(), g.end(), gamma);
     CK(cudaMemcpyAsync(d_gamma, g.data(), m * sizeof(double), cudaMemcpyHostToDevice, st));
     // gamma is staged by the copy before it returns (pageable source); the
@@ -1671,6 +1684,8 @@ struct BatchBase {
   virtual int advance(int max_steps, double tol, int* steps, double* l2) = 0;
   virtual void info(int* out) const = 0;
   virtual int tuning(int n, double* ms) const = 0;
+  virtual int snapshot(int slot, const int* which) = 0;
+  virtual int extrapolate(int n, const int* which, int* status, double* gamma) = 0;
   float last_ms = 0.f;
   std::vector<int> last_rc;  // per case: the status of the last advance
   std::vector<int> active;   // per case: 0 = left out of the advances (dgbgk_batch_set_active)
@@ -1687,6 +1702,11 @@ template <class T> struct BatchImpl : BatchBase {
   int* d_done = nullptr;
   int* h_done = nullptr;  // pinned [2]
   double* h_l2 = nullptr;  // pinned [ncases]: the cases' last L2 residuals
+  // extrapolation of the whole batch: pinned Gram matrices and coefficients
+  // [ncases][RRE_MAX^2], [ncases][RRE_MAX]; the event the cases' streams
+  // wait on after work queued on the batch's stream
+  double *h_gram = nullptr, *h_gamma = nullptr;
+  cudaEvent_t ev_q = nullptr;
   int rows = 0;           // moment rows per warp step (0: the heuristic)
   // ms per step: (eb 64, 128) x (upc 2, 4, 8, 16), then moment rows 1, 2, 3, 4;
   // 0 = not tried
@@ -1706,6 +1726,9 @@ template <class T> struct BatchImpl : BatchBase {
     dfree(d_done);
     if (h_done) cudaFreeHost(h_done);
     if (h_l2) cudaFreeHost(h_l2);
+    if (h_gram) cudaFreeHost(h_gram);
+    if (h_gamma) cudaFreeHost(h_gamma);
+    if (ev_q) cudaEventDestroy(ev_q);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     for (auto& e : evp)
@@ -1970,6 +1993,100 @@ template <class T> struct BatchImpl : BatchBase {
     return rc;
   }
 
+  // every later use of a case on its own stream follows the work just
+  // queued on the batch's stream
+  int release_to_cases(const std::vector<int>& sel) {
+    if (!ev_q) CK(cudaEventCreateWithFlags(&ev_q, cudaEventDisableTiming));
+    CK(cudaEventRecord(ev_q, st));
+    for (int i : sel) CK(cudaStreamWaitEvent(cs[i]->st, ev_q, 0));
+    return 0;
+  }
+
+  // dgbgk_snapshot(slot) of the selected cases, the copies queued on the
+  // batch's stream (no wait; the next advance follows them)
+  int snapshot(int slot, const int* which) override {
+    CK(cudaSetDevice(device));
+    if (slot < 0 || slot >= RRE_MAX) {
+      set_error("dgbgk_batch_snapshot: slot outside 0 .. " + std::to_string(RRE_MAX - 1));
+      return DGBGK_EINVAL;
+    }
+    std::vector<int> sel;
+    bool grow = false;
+    for (size_t i = 0; i < cs.size(); ++i)
+      if (!which || which[i]) {
+        sel.push_back((int)i);
+        grow |= slot >= cs[i]->snap_cap;
+      }
+    if (grow) CK(cudaStreamSynchronize(st));  // copies into the old slots land first
+    for (int i : sel) {
+      Impl<T>* c = cs[i];
+      CK(cudaStreamSynchronize(c->st));  // the case's own queued work on its state
+      if (slot >= c->snap_cap) TRY(c->grow_snaps(slot + 1));
+      const size_t N = (size_t)3 * c->pl.E * c->Vp;
+      CK(cudaMemcpyAsync(c->snaps + (size_t)slot * N, c->f[c->cur], N * sizeof(T), cudaMemcpyDeviceToDevice, st));
+    }
+    return release_to_cases(sel);
+  }
+
+  // dgbgk_extrapolate(n) of the selected cases: all Gram matrices formed
+  // before one wait, then each case's coefficients and combination
+  int extrapolate(int n, const int* which, int* status, double* gamma) override {
+    CK(cudaSetDevice(device));
+    const int m = n - 1;
+    const size_t GS = (size_t)RRE_MAX * RRE_MAX;
+    if (!h_gram) CK(cudaMallocHost((void**)&h_gram, cs.size() * GS * sizeof(double)));
+    if (!h_gamma) CK(cudaMallocHost((void**)&h_gamma, cs.size() * RRE_MAX * sizeof(double)));
+    std::vector<int> sel;
+    int rc = 0;
+    for (size_t i = 0; i < cs.size(); ++i) {
+      status[i] = 0;
+      if (which && !which[i]) continue;
+      if (n < 2 || n > cs[i]->snap_cap) {
+        status[i] = DGBGK_EINVAL;
+        set_error("dgbgk_batch_extrapolate: needs 2 <= n <= the snapshots taken");
+        if (rc == 0) rc = DGBGK_EINVAL;
+        continue;
+      }
+      sel.push_back((int)i);
+    }
+    CK(cudaStreamSynchronize(st));  // the gamma buffer's earlier copies
+    for (int i : sel) {
+      Impl<T>* c = cs[i];
+      CK(cudaStreamSynchronize(c->st));
+      if (!c->d_gram) TRY(dalloc(&c->d_gram, GS));
+      if (!c->d_gamma) TRY(dalloc(&c->d_gamma, (size_t)RRE_MAX));
+      const size_t N = (size_t)3 * c->pl.E * c->Vp;
+      CK(cudaMemsetAsync(c->d_gram, 0, (size_t)m * m * sizeof(double), st));
+      const int grid = (int)std::min<size_t>((size_t)4 * nsm, (N + 255) / 256);
+      k_gram<T><<<grid, 256, 0, st>>>(c->snaps, N, n, N, c->d_gram);
+      CK(cudaGetLastError());
+      CK(cudaMemcpyAsync(h_gram + i * GS, c->d_gram, (size_t)m * m * sizeof(double), cudaMemcpyDeviceToHost, st));
+    }
+    CK(cudaStreamSynchronize(st));
+    std::vector<int> done;
+    for (int i : sel) {
+      Impl<T>* c = cs[i];
+      std::vector<double> G(h_gram + i * GS, h_gram + i * GS + (size_t)m * m), g;
+      const int r = rre_coeffs(G, m, g);
+      status[i] = r;
+      if (r != 0) {
+        if (rc == 0) rc = r;
+        continue;
+      }
+      if (gamma) std::copy(g.begin(), g.end(), gamma + (size_t)i * m);
+      std::copy(g.begin(), g.end(), h_gamma + (size_t)i * RRE_MAX);
+      CK(cudaMemcpyAsync(c->d_gamma, h_gamma + (size_t)i * RRE_MAX, m * sizeof(double), cudaMemcpyHostToDevice, st));
+      const size_t N = (size_t)3 * c->pl.E * c->Vp;
+      const int grid = (int)std::min<size_t>((size_t)4 * nsm, (N + 255) / 256);
+      k_combine<T><<<grid, 256, 0, st>>>(c->snaps, N, m, c->d_gamma, N, c->f[c->cur]);
+      CK(cudaGetLastError());
+      ++c->epoch;
+      done.push_back(i);
+    }
+    TRY(release_to_cases(done));
+    return rc;
+  }
+
   void info(int* o) const override {
     o[0] = (int)cs.size();
     o[1] = eb;
@@ -2059,6 +2176,16 @@ int dgbgk_batch_set_active(dgbgk_batch* b, const int* active) {
   if (!b || !b->impl || !active) return set_error("NULL batch"), DGBGK_EINVAL;
   for (size_t i = 0; i < b->impl->active.size(); ++i) b->impl->active[i] = active[i] != 0;
   return DGBGK_OK;
+}
+
+int dgbgk_batch_snapshot(dgbgk_batch* b, int slot, const int* which) {
+  if (!b || !b->impl) return set_error("NULL batch"), DGBGK_EINVAL;
+  return b->impl->snapshot(slot, which);
+}
+
+int dgbgk_batch_extrapolate(dgbgk_batch* b, int n, const int* which, int* status, double* gamma) {
+  if (!b || !b->impl || !status) return set_error("NULL batch or status"), DGBGK_EINVAL;
+  return b->impl->extrapolate(n, which, status, gamma);
 }
 
 int dgbgk_batch_status(const dgbgk_batch* b, int* status) {

@@ -99,6 +99,8 @@ SIGNATURES = {
     "dgbgk_batch_create": (c_int, [POINTER(c_void_p), c_int, POINTER(BatchParams), POINTER(c_void_p)]),
     "dgbgk_batch_advance": (c_int, [c_void_p, c_int, c_double, _PI, _PD]),
     "dgbgk_batch_set_active": (c_int, [c_void_p, _PI]),
+    "dgbgk_batch_snapshot": (c_int, [c_void_p, c_int, _PI]),
+    "dgbgk_batch_extrapolate": (c_int, [c_void_p, c_int, _PI, _PI, _PD]),
     "dgbgk_batch_status": (c_int, [c_void_p, _PI]),
     "dgbgk_batch_info": (c_int, [c_void_p, _PI]),
     "dgbgk_batch_tuning": (c_int, [c_void_p, c_int, _PD]),

@@ -337,6 +337,35 @@ class Batch:
         assert a.size == len(self.solvers)
         check(lib().dgbgk_batch_set_active(self.h, ptr(a, c_int)))
 
+    def _mask(self, which):
+        if which is None:
+            return None
+        a = np.ascontiguousarray(np.asarray(which, dtype=bool).astype(np.int32))
+        assert a.size == len(self.solvers)
+        return a
+
+    def snapshot(self, slot, which=None):
+        """Solver.snapshot(slot) of the cases with which[i] true (None: all),
+        queued on the batch's stream without a wait."""
+        a = self._mask(which)
+        check(lib().dgbgk_batch_snapshot(self.h, slot, None if a is None else ptr(a, c_int)))
+
+    def extrapolate(self, n, which=None):
+        """Solver.extrapolate(n) of the cases with which[i] true (None: all),
+        their Gram matrices formed before one wait.  Returns (status, gamma):
+        per case 0 or the error code Solver.extrapolate would raise (the
+        case then keeps its state), and its n-1 coefficients (zeros where
+        not extrapolated)."""
+        a = self._mask(which)
+        k = len(self.solvers)
+        status = np.zeros(k, dtype=np.int32)
+        gamma = np.zeros((k, max(n - 1, 1)))
+        rc = lib().dgbgk_batch_extrapolate(self.h, n, None if a is None else ptr(a, c_int), ptr(status, c_int),
+                                           ptr(gamma))
+        if rc not in (0, _lib.DGBGK_EINVAL, _lib.DGBGK_ENONFINITE):
+            check(rc)  # not a case's own result (a CUDA error)
+        return status, gamma[:, :n - 1]
+
     def shape_record(self):
         """The tile shape in use: elements per CTA, units per CTA and moment
         rows per warp step."""

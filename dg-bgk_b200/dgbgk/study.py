@@ -221,7 +221,6 @@ def march_batch_rre(b, solvers, tol, max_steps, start=1e-2, every=100, m=8, stal
     from the plain march's answer; marched on plainly its residual rose to
     4e-5 and then fell to the plain answer.  A case on its way to the fixed
     point keeps falling."""
-    from ._lib import DgbgkError
     n = len(solvers)
     steps = np.zeros(n, dtype=np.int64)
     status = np.zeros(n, dtype=np.int32)
@@ -285,20 +284,19 @@ def march_batch_rre(b, solvers, tol, max_steps, start=1e-2, every=100, m=8, stal
         jumped[:] = False
         if len(act) == 0:
             continue
-        for i in act:
-            solvers[i].snapshot(0)
+        # the snapshots and the extrapolation of the whole set in batch calls
+        # (copies queued without a wait, one wait for all Gram matrices)
+        sel = np.zeros(n, dtype=bool)
+        sel[act] = True
+        b.snapshot(0, sel)
         for j in range(m + 1):
             adv(1)
-            for i in act:
-                solvers[i].snapshot(j + 1)
-        for i in act:
-            if done[i] or jumped[i]:  # finished, or its snapshots are not consecutive
-                continue
-            cyc_before[i] = rel[i]
-            try:
-                solvers[i].extrapolate(m + 2)
-            except DgbgkError:
-                use[i] = False
+            b.snapshot(j + 1, sel)
+        ext = sel & ~done & ~jumped  # not finished, snapshots consecutive
+        if ext.any():
+            cyc_before[ext] = rel[ext]
+            st, _ = b.extrapolate(m + 2, ext)
+            use[ext & (st != 0)] = False
     for s in solvers:
         s.snapshot(-1)
     b.set_active(np.ones(n, dtype=bool))

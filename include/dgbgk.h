@@ -335,6 +335,20 @@ int dgbgk_batch_tuning(const dgbgk_batch* b, int n, double* ms_per_step);
 /* Device time of the last dgbgk_batch_advance() in ms. */
 int dgbgk_batch_last_timing(const dgbgk_batch* b, double* total_ms);
 
+/* No counterpart in the reference.  dgbgk_snapshot(case, slot) of every
+ * case with which[i] non-zero (which may be NULL: all cases), the copies
+ * queued on the batch's stream without a wait; the next advance and every
+ * later use of a case follow them. */
+int dgbgk_batch_snapshot(dgbgk_batch* b, int slot, const int* which);
+
+/* dgbgk_extrapolate(case, n, ...) of every case with which[i] non-zero
+ * (NULL: all), the Gram matrices of all of them formed before one wait.
+ * status[ncases] receives each case's result (DGBGK_OK, or the code
+ * dgbgk_extrapolate would return; 0 for cases not selected; a case that
+ * fails keeps its state), gamma (may be NULL) n-1 coefficients per case at
+ * gamma[i*(n-1)].  Returns the first non-zero status. */
+int dgbgk_batch_extrapolate(dgbgk_batch* b, int n, const int* which, int* status, double* gamma);
+
 void dgbgk_batch_destroy(dgbgk_batch* b);
 
 /* ---- Warm-start network (no counterpart in the reference) ---------------

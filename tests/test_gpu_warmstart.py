@@ -161,6 +161,54 @@ def test_extrapolation_matches_numpy_rre():
     s.close()
 
 
+def numpy_rre(xs):
+    """Reduced-rank extrapolation of consecutive iterates xs in float64 (the
+    library's ridge and normalisation): the coefficients."""
+    U = np.stack([(xs[j + 1] - xs[j]).ravel() for j in range(len(xs) - 1)])
+    G = U @ U.T
+    G += 1e-14 * np.trace(G) * np.eye(len(xs) - 1)
+    g = np.linalg.solve(G, np.ones(len(xs) - 1))
+    return g / g.sum()
+
+
+@pytest.mark.parametrize("prec", [32, 64])
+def test_batch_snapshot_and_extrapolation_match_numpy_rre(prec):
+    # dgbgk_batch_snapshot / _extrapolate on two of three cases (the copies
+    # queued on the batch's stream, each case then stepping on its own
+    # stream): per selected case the coefficients and the new state equal a
+    # float64 restatement on the same iterates, as dgbgk_extrapolate's do;
+    # the case left out is untouched; a case with too few snapshots reports
+    # its error and keeps its state
+    cs = [family_case(2.5, 0.07), family_case(2.2, 0.09), family_case(2.8, 0.06)]
+    b = [cold(c, prec, 0.0, max_steps=30)[0] for c in cs]
+    batch = Batch(b, tune_steps=1)
+    which = np.array([True, False, True])
+    xs = {0: [], 2: []}
+    for j in range(5):
+        for i in xs:
+            xs[i].append(b[i].get_state())
+        batch.snapshot(j, which)
+        if j < 4:
+            for s in b:
+                s.advance(1)
+    kept = b[1].get_state()
+    st, gb = batch.extrapolate(5, which)
+    assert (st == 0).all()
+    for i in xs:
+        # an ill-conditioned system: summation order moves gamma at ~1e-7
+        np.testing.assert_allclose(gb[i], numpy_rre(xs[i]), rtol=1e-4)
+        x = np.maximum(sum(gj * xj for gj, xj in zip(gb[i], xs[i][:4])), 0.0)
+        assert rel_l2(b[i].get_state(), x) <= (1e-12 if prec == 64 else 1e-7), i
+    assert np.array_equal(b[1].get_state(), kept)
+    st, _ = batch.extrapolate(5, [False, True, False])  # case 1 took no snapshot
+    assert st[1] != 0 and st[0] == 0 and st[2] == 0
+    assert np.array_equal(b[1].get_state(), kept)
+    batch.close()
+    for s in b:
+        s.snapshot(-1)
+        s.close()
+
+
 def test_extrapolated_march_reaches_the_same_fixed_point_sooner():
     from dgbgk.study import march_batch_rre
     c = family_case(2.5, 0.07)

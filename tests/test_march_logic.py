@@ -78,6 +78,18 @@ class FakeBatch:
     def last_ms(self):
         return 0.0
 
+    def snapshot(self, slot, which=None):
+        for i, c in enumerate(self.cases):
+            if which is None or which[i]:
+                c.snapshot(slot)
+
+    def extrapolate(self, n, which=None):
+        status = np.zeros(len(self.cases), dtype=np.int32)
+        for i, c in enumerate(self.cases):
+            if which is None or which[i]:
+                c.extrapolate(n)
+        return status, np.zeros((len(self.cases), n - 1))
+
 
 def test_march_batch_stops_at_tolerance_plateau_and_divergence():
     fast = FakeCase(lambda k: 10 ** (-k / 500))                    # reaches 1e-8 at step 4000

@@ -499,9 +499,10 @@ template <class T> struct Impl : ImplBase {
   int *rside = nullptr, *rf_i = nullptr, *welem = nullptr, *spec_par = nullptr, *spec_seq_off = nullptr,
       *spec_seq = nullptr;
   T *rf_z = nullptr, *wd = nullptr;
-  // extrapolation snapshots [snap_cap][3E*Vp] and the Gram / coefficient buffers
+  // extrapolation snapshots [snap_cap][3E*Vp] (slots 0 .. snap_n - 1 taken)
+  // and the Gram / coefficient buffers
   T* snaps = nullptr;
-  int snap_cap = 0;
+  int snap_cap = 0, snap_n = 0;
   double *d_gram = nullptr, *d_gamma = nullptr;
   CaseDev<T> hc;          // this case's table entry
   LaunchSet<T> single;    // this case alone
@@ -1161,6 +1162,10 @@ template <class T> struct Impl : ImplBase {
     itime_total = 0;  // a new state: ITIME starts again
     return 0;
   }
+  // the capacity to grow to for slot `slot`: doubling (a march takes its
+  // slots in order; growing one slot at a time copied the slots taken
+  // O(m^2) times and freed and allocated device memory m times)
+  int snap_grow(int slot) const { return std::min(RRE_MAX, std::max(slot + 1, 2 * snap_cap)); }
   // room for `cap` snapshot slots, keeping the slots taken so far (the
   // caller has let every queued copy into them finish)
   int grow_snaps(int cap) {
@@ -1168,7 +1173,8 @@ template <class T> struct Impl : ImplBase {
     T* nb = nullptr;
     CK(cudaMalloc((void**)&nb, (size_t)cap * N * sizeof(T)));
     if (snaps) {
-      CK(cudaMemcpyAsync(nb, snaps, (size_t)snap_cap * N * sizeof(T), cudaMemcpyDeviceToDevice, st));
+      if (snap_n > 0)
+        CK(cudaMemcpyAsync(nb, snaps, (size_t)snap_n * N * sizeof(T), cudaMemcpyDeviceToDevice, st));
       CK(cudaStreamSynchronize(st));
       cudaFree(snaps);
     }
@@ -1182,14 +1188,15 @@ template <class T> struct Impl : ImplBase {
     if (slot < 0) {  // free the snapshots
       CK(cudaStreamSynchronize(st));
       dfree(snaps);
-      snap_cap = 0;
+      snap_cap = snap_n = 0;
       return 0;
     }
     if (slot >= RRE_MAX) {
       set_error("dgbgk_snapshot: slot beyond the extrapolation limit of " + std::to_string(RRE_MAX) + " snapshots");
       return DGBGK_EINVAL;
     }
-    if (slot >= snap_cap) TRY(grow_snaps(slot + 1));
+    if (slot >= snap_cap) TRY(grow_snaps(snap_grow(slot)));
+    snap_n = std::max(snap_n, slot + 1);
     // waited for: measured on the bench's eight channels, leaving the copy
     // queued on the case's stream made the extrapolated march slower (the
     // snapshot calls 0.20 -> 0.43 ms each)
@@ -1199,7 +1206,7 @@ template <class T> struct Impl : ImplBase {
   }
   int extrapolate(int n, double* gamma) override {
     CK(cudaSetDevice(device));
-    if (n < 2 || n > snap_cap) {
+    if (n < 2 || n > snap_n) {
       set_error("dgbgk_extrapolate: needs 2 <= n <= the snapshots taken");
       return DGBGK_EINVAL;
     }
@@ -2021,7 +2028,8 @@ template <class T> struct BatchImpl : BatchBase {
     for (int i : sel) {
       Impl<T>* c = cs[i];
       CK(cudaStreamSynchronize(c->st));  // the case's own queued work on its state
-      if (slot >= c->snap_cap) TRY(c->grow_snaps(slot + 1));
+      if (slot >= c->snap_cap) TRY(c->grow_snaps(c->snap_grow(slot)));
+      c->snap_n = std::max(c->snap_n, slot + 1);
       const size_t N = (size_t)3 * c->pl.E * c->Vp;
       CK(cudaMemcpyAsync(c->snaps + (size_t)slot * N, c->f[c->cur], N * sizeof(T), cudaMemcpyDeviceToDevice, st));
     }
@@ -2041,7 +2049,7 @@ template <class T> struct BatchImpl : BatchBase {
     for (size_t i = 0; i < cs.size(); ++i) {
       status[i] = 0;
       if (which && !which[i]) continue;
-      if (n < 2 || n > cs[i]->snap_cap) {
+      if (n < 2 || n > cs[i]->snap_n) {
         status[i] = DGBGK_EINVAL;
         set_error("dgbgk_batch_extrapolate: needs 2 <= n <= the snapshots taken");
         if (rc == 0) rc = DGBGK_EINVAL;

@@ -226,7 +226,8 @@ def channel_case(x0=-5.0, x1=15.0, y0=-5.0, y1=5.0, nx=200, ny=100, nr=24, nt=48
                    info={"mach": mach, "kn": kn, "obstacle_side": mesh.info["obstacle_side"]})
 
 
-# The benchmark workloads (sizes from the survey's scope table)
+# The benchmark workloads: the 32 x 32 lid-driven cavity, the 200 x 100
+# supersonic channel, the 400 x 200 large channel
 def config1():
     return cavity_case(32, 16, 32, mach=0.3, kn=0.1)
 

@@ -50,8 +50,9 @@ def test_create_without_gpu_fails_loudly():
 
 
 def test_another_build_of_the_abi_can_be_chosen_before_loading():
-    # `python -m dgbgk.profile --lib ...` times a compile-time variant
-    # (`make variant`); the choice is refused once a library is loaded
+    # `python -m dgbgk.profile --lib ...` times another build of the
+    # library (e.g. one compiled with other flags); the choice is refused
+    # once a library is loaded
     import subprocess
     import sys
     code = ("import dgbgk._lib as L, os; L.use_library('variant.so'); print(L.LIB_PATH); "
@@ -62,3 +63,13 @@ def test_another_build_of_the_abi_can_be_chosen_before_loading():
     assert r.returncode == 0, r.stderr
     out = r.stdout.split()
     assert out[0] == os.path.join(ROOT, "variant.so") and out[1] == "refused"
+
+
+def test_batch_extrapolation_calls_refuse_a_null_batch():
+    # argument checks before any device work (no GPU needed)
+    from dgbgk._lib import lib, DGBGK_EINVAL
+    L = lib()
+    assert L.dgbgk_batch_snapshot(None, 0, None) == DGBGK_EINVAL
+    st = (ctypes.c_int * 2)()
+    assert L.dgbgk_batch_extrapolate(None, 5, None, st, None) == DGBGK_EINVAL
+    assert b"NULL" in L.dgbgk_last_error()

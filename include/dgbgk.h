@@ -164,8 +164,8 @@ int dgbgk_copy_state(dgbgk_handle* dst, const dgbgk_handle* src);
 /* No counterpart in the reference.  Reduced-rank extrapolation of the
  * pseudo-time iterates, a way to reach the same fixed point in fewer steps:
  * dgbgk_snapshot copies the current state into slot (0 <= slot < 11; the
- * slots are allocated on the device as they are first used; slot < 0 frees
- * them).  dgbgk_extrapolate takes the snapshots x_0 .. x_{n-1} of
+ * slots' device storage grows as they are first used, doubling up to 11;
+ * slot < 0 frees them).  dgbgk_extrapolate takes the snapshots x_0 .. x_{n-1} of
  * consecutive iterates, finds gamma (n-1 values, sum 1) minimising
  * |sum_j gamma_j (x_{j+1} - x_j)|, and replaces the state by
  * max(sum_j gamma_j x_j, 0); gamma (may be NULL) receives the coefficients.

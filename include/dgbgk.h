@@ -72,7 +72,8 @@ typedef struct dgbgk_vspace {
 typedef struct dgbgk_params {
   int immat;          /* 1: lumped mass (GETINC), 0: consistent (CMMINC)  */
   double csafm;       /* Courant safety factor                            */
-  double alpha;       /* wall accommodation (1 = fully diffuse; < 1 needs immat = 1) */
+  double alpha;       /* wall accommodation (1 = fully diffuse; < 1 adds the
+                         specular part, with either immat)                 */
   double rgas;        /* gas constant R                                   */
   double molar_mass;  /* M                                                */
   double diameter;    /* molecular diameter d                             */

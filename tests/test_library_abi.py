@@ -73,3 +73,23 @@ def test_batch_extrapolation_calls_refuse_a_null_batch():
     st = (ctypes.c_int * 2)()
     assert L.dgbgk_batch_extrapolate(None, 5, None, st, None) == DGBGK_EINVAL
     assert b"NULL" in L.dgbgk_last_error()
+
+
+def declared_arity():
+    """Parameter count of every dgbgk_* function the header declares."""
+    src = open(os.path.join(ROOT, "include", "dgbgk.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    out = {}
+    for m in re.finditer(r"\b(dgbgk_\w+)\s*\(([^;{]*?)\)\s*;", src, flags=re.S):
+        args = " ".join(m.group(2).split())
+        out[m.group(1)] = 0 if args in ("", "void") else args.count(",") + 1
+    return out
+
+
+def test_python_binding_takes_the_header_arguments():
+    # the ctypes argument lists match the C declarations one for one
+    from dgbgk import _lib
+    ar = declared_arity()
+    assert set(ar) == set(declared())
+    wrong = {n: (k, len(_lib.SIGNATURES[n][1])) for n, k in ar.items() if len(_lib.SIGNATURES[n][1]) != k}
+    assert not wrong, wrong
